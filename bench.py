@@ -1,0 +1,303 @@
+"""Benchmark: SCC decomposition throughput (GTEPS) on one B200 per rank.
+
+Workload (default): the large mixed-structure graph -- the union of a directed
+R-MAT scale-24 graph (edge factor 16, a/b/c/d = .57/.19/.19/.05) and a
+4096 x 4096 grid whose edges are oriented by a fair coin with 5% made
+bidirectional; self-loops and duplicates removed; seeded synthetic data.
+A step is one full SCC decomposition (method 2: Trim1 + global FW-BW +
+Trim1/2 + WCC + FW-BW) of that graph, inputs resident in HBM (the CSR and its
+transpose are 2.5 GB, far above the 126 MB L2, so no flush is needed).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2|rmat24|c1]
+
+Prints one JSON line (rank 0).  value = whole-job GTEPS = edges of all ranks'
+graphs / max-over-ranks device time per step; e2e = the same metric through
+the C ABI from pinned host CSR arrays (H2D of the CSR + transpose, run, D2H of
+the canonical labels inside the timed region).  --gpus N > 1 runs N
+independent replicas (the path does not shard; no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "c2": dict(rmat_scale=24, edge_factor=16, grid_side=4096, seed=2024),
+    "rmat24": dict(rmat_scale=24, edge_factor=16, seed=2024),
+    "c1": dict(rmat_scale=16, edge_factor=8, seed=42),
+}
+# CPU-baseline sample of the same workload shape at 1/16 of the vertices
+CPU_SAMPLES = {
+    "c2": dict(rmat_scale=20, edge_factor=16, grid_side=1024, seed=2024),
+    "rmat24": dict(rmat_scale=20, edge_factor=16, seed=2024),
+    "c1": dict(rmat_scale=16, edge_factor=8, seed=42),
+}
+WORKLOAD_NAMES = {
+    "c2": "R-MAT s24 ef16 (a=.57,b=.19,c=.19) U 4096x4096 randomly oriented grid (+5% bidirectional)",
+    "rmat24": "R-MAT s24 ef16 (a=.57,b=.19,c=.19)",
+    "c1": "R-MAT s16 ef8 (a=.57,b=.19,c=.19)",
+}
+
+
+def measured_peak_gbs():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+        sm = []
+        mx = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for p in self.samples:
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, p[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(args, workload):
+    """Reference arm: the reference's own OpenMP method-2 pipeline on the host cores."""
+    from oracle import oracle as O
+    from dynamicgraphs_scc_b200 import generate_edges_host
+    kw = CPU_SAMPLES[workload]
+    n, s, d = generate_edges_host(**kw)
+    s, d = O.dedup_edges(s, d)
+    csr = O.build_csr(n, s, d)
+    threads = os.cpu_count() or 1
+    kind = "reference" if O.ref_available() else "port"
+    times = []
+    for i in range(args.warmup + args.steps):
+        if kind == "reference":
+            _, ms = O.ref_method2(csr, threads=threads)
+        else:
+            t0 = time.perf_counter()
+            O.tarjan_canonical(csr[0], csr[1])
+            ms = (time.perf_counter() - t0) * 1e3
+        if i >= args.warmup:
+            times.append(ms)
+    ms = statistics.mean(times)
+    gteps = s.size / (ms * 1e-3) / 1e9
+    sample = f"{WORKLOAD_NAMES[workload]} scaled to " + json.dumps(kw) + f": n={n} m={s.size}"
+    return gteps, ms, dict(value=gteps, unit="GTEPS", cores=threads if kind == "reference" else 1, kind=kind,
+                           sample=sample, ms=ms)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        gteps, ms, cpu = run_reference(args, args.workload)
+        line = {"metric": "SCC GTEPS (edges / end-to-end decomposition time)", "value": round(gteps, 6),
+                "unit": "GTEPS", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
+                "config": {"workload": WORKLOAD_NAMES[args.workload], "sample": cpu["sample"],
+                           "method": 2, "parallelism": f"replicas x{args.gpus}"},
+                "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": round(gteps, 6), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local_rank)
+    from dynamicgraphs_scc_b200 import Graph, State, capi
+
+    kw = WORKLOADS[args.workload]
+    g = Graph.generate(**kw, device=local_rank)
+    n, m = g.num_nodes(), g.num_edges()
+    st = State(g)
+    stream = torch.cuda.ExternalStream(st.stream(), device=local_rank)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        st.reset()
+        st.run(2)
+    st.synchronize()
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    kernels = 0
+    per_step = []
+    phase = []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        st.reset()
+        stats = st.run(2)
+        kernels += stats["kernels_launched"] + 3
+        per_step.append(stats["ms_total"])
+        phase.append(stats)
+    ev1.record(stream)
+    st.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_edges = m * world
+    gteps = total_edges / (ms * 1e-3) / 1e9
+
+    # roofline of the whole step (algorithmic bytes 16M + 20N + 8)
+    peak, peak_kind = measured_peak_gbs()
+    b_alg = 16 * m + 20 * n + 8
+    achieved = b_alg / (ms * 1e-3) / 1e9
+
+    # e2e: host CSR (pinned) -> H2D -> run -> canonical labels D2H, through the C ABI
+    b, a, rb, ra = g.csr()
+    hb = torch.from_numpy(b).pin_memory(); ha = torch.from_numpy(a).pin_memory()
+    hrb = torch.from_numpy(rb).pin_memory(); hra = torch.from_numpy(ra).pin_memory()
+    labels = torch.empty(n, dtype=torch.int32).pin_memory()
+    lib = capi.lib()
+    e2e_ms = []
+    for i in range(args.e2e_steps + 1):
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        capi.call("scc_graph_upload_csr", g.handle, hb.data_ptr(), ha.data_ptr(), hrb.data_ptr(), hra.data_ptr(),
+                  st.stream())
+        st.reset()
+        st.run(2)
+        capi.call("scc_canonical_labels", st.handle, C.cast(labels.data_ptr(), C.POINTER(C.c_int32)))
+        e1.record(stream)
+        st.synchronize()
+        if i > 0:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e = statistics.mean(e2e_ms)
+    if dist is not None:
+        t = torch.tensor([e2e], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = float(t.item())
+    e2e_gteps = total_edges / (e2e * 1e-3) / 1e9
+    h2d = 4 * (2 * (n + 1) + 2 * m)
+    d2h = 4 * n
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            _, _, cpu = run_reference(argparse.Namespace(steps=1, warmup=0), args.workload)
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as exc:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": "GTEPS", "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    last = phase[-1]
+    line = {
+        "metric": "SCC GTEPS (edges / end-to-end decomposition time)",
+        "value": round(gteps, 4), "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic (seeded generator, same shapes as the benchmark configuration)",
+        "config": {"workload": WORKLOAD_NAMES[args.workload], "params": kw, "n": n, "m": m, "method": 2,
+                   "pivot": "max in*out degree", "parallelism": f"replicas x{world}",
+                   "l2": "inputs (CSR+transpose) > L2; no flush"},
+        "roofline": {"bound": "hbm", "scope": "whole step (16M+20N+8 algorithmic bytes)",
+                     "achieved": round(achieved, 2), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / peak, 5), "traffic": None},
+        "e2e": {"value": round(e2e_gteps, 4), "unit": "GTEPS", "ms_per_step": round(e2e, 3),
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": kernels,
+        "phases_ms": {k: round(last[k], 3) for k in ("ms_trim1", "ms_global_fb", "ms_trim12", "ms_wcc", "ms_fb")},
+        "stats": {k: last[k] for k in ("num_sccs", "first_scc_size", "trimmed_first", "trimmed_second",
+                                        "num_wcc_classes", "traversal_steps")},
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

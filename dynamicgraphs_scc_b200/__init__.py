@@ -1,0 +1,14 @@
+"""B200-native strongly-connected-components engine.
+
+A drop-in for the SCC path of ShashwaTTrigunayaT/DynamicGraphs_SCC: the
+reference's phase API (trim1 / trim2 / FW-BW / WCC / colour / work queue /
+driver) over device-resident int32 CSR, computed by hand-written sm_100a
+kernels behind a C ABI (include/scc_capi.h).
+"""
+from .capi import SccError, lib  # noqa: F401
+from .engine import (  # noqa: F401
+    METHOD_BASELINE, METHOD_GLOBAL_FB, METHOD_GLOBAL_WCC_FB, PIVOT_DEGREE, PIVOT_LEARNED,
+    Graph, State, decompose_csr, device_count, gen_params, generate_edges_host, read_scc_list,
+)
+
+__version__ = "0.1.0"

@@ -1,0 +1,426 @@
+// Graph construction: edge list -> sorted CSR + sorted transpose, on the device.
+//
+// Replaces gm_graph add_node/add_edge + freeze + do_semi_sort +
+// make_reverse_edges (gm_graph/src/gm_graph.cc:459-480, 60-101, 385-420,
+// 193-287): one 64-bit radix sort of (src<<32 | dst) keys gives the out-CSR
+// with each adjacency list sorted by destination (the semi-sort), a second
+// sort of (dst<<32 | src) gives the transpose sorted by source.  Offsets are
+// filled from the sorted keys by a gap-fill kernel.  Duplicates and self-loops
+// are kept unless the caller asks otherwise, as gm_graph keeps them.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_select.cuh>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+#include "scc_internal.cuh"
+
+// ------------------------------------------------------------------ errors
+static thread_local char g_err[512] = "";
+
+void scc_set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+int scc_cuda_status(cudaError_t e, const char* what, const char* file, int line) {
+    scc_set_error("CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e), what, file, line);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();  // clear the sticky-free allocation error
+        return SCC_ERR_OOM;
+    }
+    return SCC_ERR_CUDA;
+}
+
+extern "C" const char* scc_last_error(void) { return g_err; }
+
+extern "C" const char* scc_status_string(int status) {
+    switch (status) {
+        case SCC_OK: return "ok";
+        case SCC_ERR_INVALID: return "invalid argument";
+        case SCC_ERR_CUDA: return "CUDA error";
+        case SCC_ERR_OOM: return "out of device memory";
+        case SCC_ERR_TIMEOUT: return "bounded device wait gave up";
+        case SCC_ERR_STATE: return "call out of order";
+        case SCC_ERR_IO: return "file error";
+        case SCC_ERR_NOT_FOUND: return "not found";
+        case SCC_ERR_UNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int scc_version(void) { return 100; }
+
+extern "C" int scc_device_count(int* count) {
+    SCC_REQUIRE(count, SCC_ERR_INVALID, "count is NULL");
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) { cudaGetLastError(); c = 0; }
+    *count = c;
+    return SCC_OK;
+}
+
+// ------------------------------------------------------------------ kernels
+__global__ void k_make_keys(int64_t m, const int32_t* __restrict__ a, const int32_t* __restrict__ b,
+                            unsigned long long* __restrict__ keys, int drop_self,
+                            unsigned long long* __restrict__ dropped) {
+    unsigned long long local = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t x = (uint32_t)a[i], y = (uint32_t)b[i];
+        if (drop_self && x == y) { keys[i] = ~0ull; local++; }
+        else keys[i] = ((unsigned long long)x << 32) | y;
+    }
+    if (local) atomicAdd(dropped, local);
+}
+
+// begin[v] = first index i with key[i]>>32 >= v, for v in [0, n]; keys sorted.
+__global__ void k_fill_offsets(int64_t m, int32_t n, const unsigned long long* __restrict__ keys,
+                               int32_t* __restrict__ begin) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= m; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t prev = (i == 0) ? -1 : (int64_t)(keys[i - 1] >> 32);
+        int64_t cur = (i == m) ? (int64_t)n : (int64_t)(keys[i] >> 32);
+        for (int64_t v = prev + 1; v <= cur && v <= n; ++v) begin[v] = (int32_t)i;
+    }
+}
+
+__global__ void k_low_words(int64_t m, const unsigned long long* __restrict__ keys, int32_t* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (int32_t)(uint32_t)(keys[i] & 0xFFFFFFFFull);
+}
+
+// src[e] = v for e in [begin[v], begin[v+1]) -- one warp per vertex.
+__global__ void k_expand_sources(int32_t n, const int32_t* __restrict__ begin, int32_t* __restrict__ src) {
+    int lane = threadIdx.x & 31;
+    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < n;
+         w += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int32_t b = begin[w], e = begin[w + 1];
+        for (int32_t k = b + lane; k < e; k += 32) src[k] = (int32_t)w;
+    }
+}
+
+__global__ void k_check_ids(int64_t m, int32_t n, const int32_t* __restrict__ a, const int32_t* __restrict__ b,
+                            int* __restrict__ bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        if (a[i] < 0 || a[i] >= n || b[i] < 0 || b[i] >= n) { atomicExch(bad, 1); return; }
+    }
+}
+
+static int bits_for(int32_t n) {
+    int b = 1;
+    while (b < 31 && (1LL << b) < (int64_t)n) b++;
+    return b;
+}
+
+// Sort (hi<<32|lo) keys and write offsets + low words.  keys buffer is reused.
+static int build_side(int32_t n, int64_t m, const int32_t* hi, const int32_t* lo, int flags, cudaStream_t st,
+                      int32_t** begin_out, int32_t** idx_out, int64_t* m_out) {
+    unsigned long long *keys = nullptr, *keys2 = nullptr, *dropped = nullptr;
+    int64_t mm = m > 0 ? m : 1;
+    SCC_CUDA(cudaMalloc(&keys, sizeof(unsigned long long) * mm));
+    cudaError_t e1 = cudaMalloc(&keys2, sizeof(unsigned long long) * mm);
+    if (e1 != cudaSuccess) { cudaFree(keys); return scc_cuda_status(e1, "cudaMalloc keys2", __FILE__, __LINE__); }
+    SCC_CUDA(cudaMalloc(&dropped, sizeof(unsigned long long) * 2));
+    SCC_CUDA(cudaMemsetAsync(dropped, 0, sizeof(unsigned long long) * 2, st));
+    int drop_self = (flags & SCC_BUILD_NO_SELF_LOOPS) ? 1 : 0;
+    if (m > 0) {
+        k_make_keys<<<scc_blocks(m, 256, 148 * 64), 256, 0, st>>>(m, hi, lo, keys, drop_self, dropped);
+        SCC_CUDA(cudaPeekAtLastError());
+    }
+    int end_bit = 32 + bits_for(n + 1);
+    if (drop_self) end_bit = 64;
+    size_t tmp_bytes = 0;
+    void* tmp = nullptr;
+    cub::DoubleBuffer<unsigned long long> db(keys, keys2);
+    SCC_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, (int)m, 0, end_bit, st));
+    SCC_CUDA(cudaMalloc(&tmp, tmp_bytes > 0 ? tmp_bytes : 16));
+    if (m > 0) SCC_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, (int)m, 0, end_bit, st));
+    cudaFree(tmp);
+    unsigned long long* sorted = db.Current();
+    unsigned long long* other = db.Alternate();
+    unsigned long long h_dropped = 0;
+    SCC_CUDA(cudaMemcpyAsync(&h_dropped, dropped, sizeof(h_dropped), cudaMemcpyDeviceToHost, st));
+    SCC_CUDA(cudaStreamSynchronize(st));
+    int64_t mk = m - (int64_t)h_dropped;   // self-loops sorted to the end
+    if ((flags & SCC_BUILD_DEDUP) && mk > 0) {
+        int* d_num = nullptr;
+        SCC_CUDA(cudaMalloc(&d_num, sizeof(int)));
+        tmp_bytes = 0;
+        SCC_CUDA(cub::DeviceSelect::Unique(nullptr, tmp_bytes, sorted, other, d_num, (int)mk, st));
+        SCC_CUDA(cudaMalloc(&tmp, tmp_bytes > 0 ? tmp_bytes : 16));
+        SCC_CUDA(cub::DeviceSelect::Unique(tmp, tmp_bytes, sorted, other, d_num, (int)mk, st));
+        int h_num = 0;
+        SCC_CUDA(cudaMemcpyAsync(&h_num, d_num, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SCC_CUDA(cudaStreamSynchronize(st));
+        cudaFree(tmp); cudaFree(d_num);
+        mk = h_num;
+        unsigned long long* t = sorted; sorted = other; other = t;
+    }
+    int32_t *begin = nullptr, *idx = nullptr;
+    SCC_CUDA(cudaMalloc(&begin, sizeof(int32_t) * ((size_t)n + 1)));
+    SCC_CUDA(cudaMalloc(&idx, sizeof(int32_t) * (size_t)(mk > 0 ? mk : 1)));
+    k_fill_offsets<<<scc_blocks(mk + 1, 256, 148 * 64), 256, 0, st>>>(mk, n, sorted, begin);
+    SCC_CUDA(cudaPeekAtLastError());
+    if (mk > 0) {
+        k_low_words<<<scc_blocks(mk, 256, 148 * 64), 256, 0, st>>>(mk, sorted, idx);
+        SCC_CUDA(cudaPeekAtLastError());
+    }
+    SCC_CUDA(cudaStreamSynchronize(st));
+    cudaFree(keys); cudaFree(keys2); cudaFree(dropped);
+    *begin_out = begin; *idx_out = idx; *m_out = mk;
+    return SCC_OK;
+}
+
+int scc_impl_build_graph_from_device_edges(int32_t n, int64_t m, const int32_t* d_src, const int32_t* d_dst,
+                                           int flags, int device, scc_graph** out) {
+    SCC_REQUIRE(out, SCC_ERR_INVALID, "out is NULL");
+    SCC_REQUIRE(n >= 0 && m >= 0, SCC_ERR_INVALID, "negative size n=%d m=%lld", n, (long long)m);
+    SCC_REQUIRE(m < (1LL << 31) - 1, SCC_ERR_INVALID, "m=%lld exceeds int32 edge ids", (long long)m);
+    SCC_REQUIRE(n < SCC_WCC_ROOT_MASK, SCC_ERR_INVALID, "n=%d exceeds 0x1FFFFFFF", n);
+    SCC_CUDA(cudaSetDevice(device));
+    cudaStream_t st;
+    SCC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    if (m > 0) {
+        int* bad = nullptr;
+        SCC_CUDA(cudaMalloc(&bad, sizeof(int)));
+        SCC_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), st));
+        k_check_ids<<<scc_blocks(m, 256, 148 * 64), 256, 0, st>>>(m, n, d_src, d_dst, bad);
+        int hb = 0;
+        SCC_CUDA(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SCC_CUDA(cudaStreamSynchronize(st));
+        cudaFree(bad);
+        if (hb) { cudaStreamDestroy(st); scc_set_error("edge endpoint outside [0, %d)", n); return SCC_ERR_INVALID; }
+    }
+    scc_graph* g = new scc_graph();
+    g->device = device;
+    g->n = n;
+    int64_t m1 = 0, m2 = 0;
+    int s = build_side(n, m, d_src, d_dst, flags, st, &g->begin, &g->node_idx, &m1);
+    if (s == SCC_OK) s = build_side(n, m, d_dst, d_src, flags, st, &g->r_begin, &g->r_node_idx, &m2);
+    cudaStreamDestroy(st);
+    if (s != SCC_OK) { scc_graph_free(g); return s; }
+    g->m = m1;
+    *out = g;
+    return SCC_OK;
+}
+
+int scc_impl_transpose(scc_graph* g, cudaStream_t st) {
+    int32_t* src = nullptr;
+    SCC_CUDA(cudaMalloc(&src, sizeof(int32_t) * (size_t)(g->m > 0 ? g->m : 1)));
+    k_expand_sources<<<scc_blocks((int64_t)g->n * 32, 256, 148 * 64), 256, 0, st>>>(g->n, g->begin, src);
+    SCC_CUDA(cudaPeekAtLastError());
+    int64_t m2 = 0;
+    int s = build_side(g->n, g->m, g->node_idx, src, SCC_BUILD_KEEP_ALL, st, &g->r_begin, &g->r_node_idx, &m2);
+    cudaFree(src);
+    return s;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" int scc_graph_create_edges_device(int32_t n, int64_t m, const int32_t* d_src, const int32_t* d_dst,
+                                             int flags, int device, scc_graph** out) {
+    SCC_REQUIRE(m == 0 || (d_src && d_dst), SCC_ERR_INVALID, "edge arrays are NULL");
+    return scc_impl_build_graph_from_device_edges(n, m, d_src, d_dst, flags, device, out);
+}
+
+extern "C" int scc_graph_create_edges(int32_t n, int64_t m, const int32_t* src, const int32_t* dst, int flags,
+                                      int device, scc_graph** out) {
+    SCC_REQUIRE(m == 0 || (src && dst), SCC_ERR_INVALID, "edge arrays are NULL");
+    SCC_REQUIRE(m >= 0 && n >= 0, SCC_ERR_INVALID, "negative size");
+    SCC_CUDA(cudaSetDevice(device));
+    int32_t *ds = nullptr, *dd = nullptr;
+    size_t bytes = sizeof(int32_t) * (size_t)(m > 0 ? m : 1);
+    SCC_CUDA(cudaMalloc(&ds, bytes));
+    cudaError_t e = cudaMalloc(&dd, bytes);
+    if (e != cudaSuccess) { cudaFree(ds); return scc_cuda_status(e, "cudaMalloc", __FILE__, __LINE__); }
+    if (m > 0) {
+        SCC_CUDA(cudaMemcpy(ds, src, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice));
+        SCC_CUDA(cudaMemcpy(dd, dst, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice));
+    }
+    int s = scc_impl_build_graph_from_device_edges(n, m, ds, dd, flags, device, out);
+    cudaFree(ds); cudaFree(dd);
+    return s;
+}
+
+static int create_csr_common(int32_t n, int32_t m, const int32_t* begin, const int32_t* node_idx,
+                             const int32_t* r_begin, const int32_t* r_node_idx, int device, scc_graph** out,
+                             cudaMemcpyKind kind) {
+    SCC_REQUIRE(out, SCC_ERR_INVALID, "out is NULL");
+    SCC_REQUIRE(n >= 0 && m >= 0, SCC_ERR_INVALID, "negative size");
+    SCC_REQUIRE(begin && (m == 0 || node_idx), SCC_ERR_INVALID, "CSR arrays are NULL");
+    SCC_REQUIRE((r_begin == nullptr) == (r_node_idx == nullptr) || m == 0, SCC_ERR_INVALID,
+                "give both transpose arrays or neither");
+    SCC_REQUIRE(n < SCC_WCC_ROOT_MASK, SCC_ERR_INVALID, "n=%d exceeds 0x1FFFFFFF", n);
+    SCC_CUDA(cudaSetDevice(device));
+    scc_graph* g = new scc_graph();
+    g->device = device; g->n = n; g->m = m;
+    size_t nb = sizeof(int32_t) * ((size_t)n + 1), mb = sizeof(int32_t) * (size_t)(m > 0 ? m : 1);
+    cudaError_t e = cudaMalloc(&g->begin, nb);
+    if (e == cudaSuccess) e = cudaMalloc(&g->node_idx, mb);
+    if (e == cudaSuccess) e = cudaMemcpy(g->begin, begin, nb, kind);
+    if (e == cudaSuccess && m > 0) e = cudaMemcpy(g->node_idx, node_idx, sizeof(int32_t) * (size_t)m, kind);
+    if (e == cudaSuccess && r_begin) {
+        e = cudaMalloc(&g->r_begin, nb);
+        if (e == cudaSuccess) e = cudaMalloc(&g->r_node_idx, mb);
+        if (e == cudaSuccess) e = cudaMemcpy(g->r_begin, r_begin, nb, kind);
+        if (e == cudaSuccess && m > 0) e = cudaMemcpy(g->r_node_idx, r_node_idx, sizeof(int32_t) * (size_t)m, kind);
+    }
+    if (e != cudaSuccess) { scc_graph_free(g); return scc_cuda_status(e, "csr upload", __FILE__, __LINE__); }
+    if (!r_begin) {
+        cudaStream_t st;
+        SCC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        int s = scc_impl_transpose(g, st);
+        cudaStreamDestroy(st);
+        if (s != SCC_OK) { scc_graph_free(g); return s; }
+    }
+    *out = g;
+    return SCC_OK;
+}
+
+extern "C" int scc_graph_create_csr(int32_t n, int32_t m, const int32_t* begin, const int32_t* node_idx,
+                                    const int32_t* r_begin, const int32_t* r_node_idx, int device, scc_graph** out) {
+    return create_csr_common(n, m, begin, node_idx, r_begin, r_node_idx, device, out, cudaMemcpyHostToDevice);
+}
+
+extern "C" int scc_graph_create_csr_device(int32_t n, int32_t m, const int32_t* d_begin, const int32_t* d_node_idx,
+                                           const int32_t* d_r_begin, const int32_t* d_r_node_idx, int device,
+                                           scc_graph** out) {
+    return create_csr_common(n, m, d_begin, d_node_idx, d_r_begin, d_r_node_idx, device, out,
+                             cudaMemcpyDeviceToDevice);
+}
+
+extern "C" int scc_graph_upload_csr(scc_graph* g, const int32_t* begin, const int32_t* node_idx,
+                                    const int32_t* r_begin, const int32_t* r_node_idx, void* stream) {
+    SCC_REQUIRE(g && begin && r_begin && (g->m == 0 || (node_idx && r_node_idx)), SCC_ERR_INVALID, "NULL argument");
+    SCC_CUDA(cudaSetDevice(g->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t nb = sizeof(int32_t) * ((size_t)g->n + 1), mb = sizeof(int32_t) * (size_t)g->m;
+    SCC_CUDA(cudaMemcpyAsync(g->begin, begin, nb, cudaMemcpyHostToDevice, st));
+    SCC_CUDA(cudaMemcpyAsync(g->r_begin, r_begin, nb, cudaMemcpyHostToDevice, st));
+    if (g->m > 0) {
+        SCC_CUDA(cudaMemcpyAsync(g->node_idx, node_idx, mb, cudaMemcpyHostToDevice, st));
+        SCC_CUDA(cudaMemcpyAsync(g->r_node_idx, r_node_idx, mb, cudaMemcpyHostToDevice, st));
+    }
+    return SCC_OK;
+}
+
+extern "C" int scc_graph_free(scc_graph* g) {
+    if (!g) return SCC_OK;
+    cudaSetDevice(g->device);
+    if (g->owns) {
+        cudaFree(g->begin); cudaFree(g->node_idx); cudaFree(g->r_begin); cudaFree(g->r_node_idx);
+    }
+    delete g;
+    return SCC_OK;
+}
+
+extern "C" int scc_graph_num_nodes(const scc_graph* g, int32_t* n) {
+    SCC_REQUIRE(g && n, SCC_ERR_INVALID, "NULL argument");
+    *n = g->n;
+    return SCC_OK;
+}
+
+extern "C" int scc_graph_num_edges(const scc_graph* g, int64_t* m) {
+    SCC_REQUIRE(g && m, SCC_ERR_INVALID, "NULL argument");
+    *m = g->m;
+    return SCC_OK;
+}
+
+extern "C" int scc_graph_copy_csr(const scc_graph* g, int32_t* begin, int32_t* node_idx, int32_t* r_begin,
+                                  int32_t* r_node_idx) {
+    SCC_REQUIRE(g, SCC_ERR_INVALID, "graph is NULL");
+    SCC_CUDA(cudaSetDevice(g->device));
+    size_t nb = sizeof(int32_t) * ((size_t)g->n + 1), mb = sizeof(int32_t) * (size_t)g->m;
+    if (begin) SCC_CUDA(cudaMemcpy(begin, g->begin, nb, cudaMemcpyDeviceToHost));
+    if (r_begin) SCC_CUDA(cudaMemcpy(r_begin, g->r_begin, nb, cudaMemcpyDeviceToHost));
+    if (g->m > 0) {
+        if (node_idx) SCC_CUDA(cudaMemcpy(node_idx, g->node_idx, mb, cudaMemcpyDeviceToHost));
+        if (r_node_idx) SCC_CUDA(cudaMemcpy(r_node_idx, g->r_node_idx, mb, cudaMemcpyDeviceToHost));
+    }
+    return SCC_OK;
+}
+
+extern "C" int scc_graph_device_csr(const scc_graph* g, const int32_t** d_begin, const int32_t** d_node_idx,
+                                    const int32_t** d_r_begin, const int32_t** d_r_node_idx) {
+    SCC_REQUIRE(g, SCC_ERR_INVALID, "graph is NULL");
+    if (d_begin) *d_begin = g->begin;
+    if (d_node_idx) *d_node_idx = g->node_idx;
+    if (d_r_begin) *d_r_begin = g->r_begin;
+    if (d_r_node_idx) *d_r_node_idx = g->r_node_idx;
+    return SCC_OK;
+}
+
+// ------------------------------------------------------------------ files
+extern "C" int scc_graph_save_binary(const scc_graph* g, const char* path) {
+    SCC_REQUIRE(g && path, SCC_ERR_INVALID, "NULL argument");
+    std::vector<int32_t> b((size_t)g->n + 1), a((size_t)g->m);
+    SCC_TRY(scc_graph_copy_csr(g, b.data(), a.data(), nullptr, nullptr));
+    FILE* f = fopen(path, "wb");
+    SCC_REQUIRE(f, SCC_ERR_IO, "cannot open %s for writing", path);
+    int64_t hdr[2] = {g->n, g->m};
+    bool ok = fwrite("SCCCSR01", 1, 8, f) == 8 && fwrite(hdr, sizeof(hdr), 1, f) == 1 &&
+              fwrite(b.data(), sizeof(int32_t), b.size(), f) == b.size() &&
+              fwrite(a.data(), sizeof(int32_t), a.size(), f) == a.size();
+    fclose(f);
+    SCC_REQUIRE(ok, SCC_ERR_IO, "short write to %s", path);
+    return SCC_OK;
+}
+
+extern "C" int scc_graph_load_binary(const char* path, int device, scc_graph** out) {
+    SCC_REQUIRE(path && out, SCC_ERR_INVALID, "NULL argument");
+    FILE* f = fopen(path, "rb");
+    SCC_REQUIRE(f, SCC_ERR_IO, "cannot open %s", path);
+    char magic[8];
+    int64_t hdr[2];
+    if (fread(magic, 1, 8, f) != 8 || memcmp(magic, "SCCCSR01", 8) != 0 || fread(hdr, sizeof(hdr), 1, f) != 1 ||
+        hdr[0] < 0 || hdr[1] < 0 || hdr[0] >= SCC_WCC_ROOT_MASK || hdr[1] >= (1LL << 31)) {
+        fclose(f);
+        scc_set_error("%s is not an SCC binary CSR file", path);
+        return SCC_ERR_IO;
+    }
+    std::vector<int32_t> b((size_t)hdr[0] + 1), a((size_t)hdr[1]);
+    bool ok = fread(b.data(), sizeof(int32_t), b.size(), f) == b.size() &&
+              fread(a.data(), sizeof(int32_t), a.size(), f) == a.size();
+    fclose(f);
+    SCC_REQUIRE(ok, SCC_ERR_IO, "truncated file %s", path);
+    return scc_graph_create_csr((int32_t)hdr[0], (int32_t)hdr[1], b.data(), a.data(), nullptr, nullptr, device, out);
+}
+
+// Fast text parser: "u v" per line, 1-based; N = max id (src/common_main.h:61-83,
+// src_CUDA/scc_cuda_dynamic.cpp:59-147).
+extern "C" int scc_graph_load_edge_list(const char* path, int device, scc_graph** out) {
+    SCC_REQUIRE(path && out, SCC_ERR_INVALID, "NULL argument");
+    FILE* f = fopen(path, "rb");
+    SCC_REQUIRE(f, SCC_ERR_IO, "cannot open %s", path);
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    std::vector<char> buf((size_t)(sz > 0 ? sz : 0) + 1);
+    size_t rd = sz > 0 ? fread(buf.data(), 1, (size_t)sz, f) : 0;
+    fclose(f);
+    buf[rd] = 0;
+    std::vector<int32_t> src, dst;
+    int64_t maxid = 0;
+    const char* p = buf.data();
+    const char* end = p + rd;
+    while (p < end) {
+        while (p < end && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n')) p++;
+        if (p >= end) break;
+        if (*p == '%' || *p == '#') { while (p < end && *p != '\n') p++; continue; }
+        int64_t v[2];
+        for (int k = 0; k < 2; ++k) {
+            while (p < end && (*p == ' ' || *p == '\t')) p++;
+            if (p >= end || *p < '0' || *p > '9') { scc_set_error("%s: malformed line", path); return SCC_ERR_IO; }
+            int64_t x = 0;
+            while (p < end && *p >= '0' && *p <= '9') { x = x * 10 + (*p - '0'); p++; if (x > 0x7FFFFFFF) break; }
+            if (x < 1 || x > 0x1FFFFFFE) { scc_set_error("%s: vertex id %lld out of range", path, (long long)x); return SCC_ERR_IO; }
+            v[k] = x;
+        }
+        while (p < end && *p != '\n') p++;
+        src.push_back((int32_t)(v[0] - 1));
+        dst.push_back((int32_t)(v[1] - 1));
+        if (v[0] > maxid) maxid = v[0];
+        if (v[1] > maxid) maxid = v[1];
+    }
+    return scc_graph_create_edges((int32_t)maxid, (int64_t)src.size(), src.data(), dst.data(), SCC_BUILD_KEEP_ALL,
+                                  device, out);
+}

@@ -1,0 +1,135 @@
+// Internal definitions shared by the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string>
+#include <vector>
+#include "scc_capi.h"
+
+// ---------------------------------------------------------------- error plumbing
+void scc_set_error(const char* fmt, ...);
+int scc_cuda_status(cudaError_t e, const char* what, const char* file, int line);
+
+#define SCC_CUDA(call)                                                            \
+    do {                                                                          \
+        cudaError_t _e = (call);                                                  \
+        if (_e != cudaSuccess) return scc_cuda_status(_e, #call, __FILE__, __LINE__); \
+    } while (0)
+#define SCC_TRY(call)                                                             \
+    do { int _s = (call); if (_s != SCC_OK) return _s; } while (0)
+#define SCC_REQUIRE(cond, code, ...)                                              \
+    do { if (!(cond)) { scc_set_error(__VA_ARGS__); return (code); } } while (0)
+// launch check: cudaGetLastError after each launch
+#define SCC_LAUNCHED(st) SCC_CUDA(cudaPeekAtLastError()); (st)->kernels++
+
+// ---------------------------------------------------------------- constants
+#define SCC_THREADS 256
+#define SCC_WCC_HIGH_DEG_FLAG 0x20000000   // scc_weak.cc:141-146
+#define SCC_WCC_ROOT_MASK 0x1FFFFFFF
+#define SCC_WCC_HIGH_DEG 50                // scc_weak.cc:143
+
+// ---------------------------------------------------------------- graph
+struct scc_graph {
+    int device = 0;
+    int32_t n = 0;
+    int64_t m = 0;
+    int32_t* begin = nullptr;     // [n+1]  out-CSR offsets      (gm_graph::begin)
+    int32_t* node_idx = nullptr;  // [m]    out-neighbours       (gm_graph::node_idx)
+    int32_t* r_begin = nullptr;   // [n+1]  in-CSR offsets       (gm_graph::r_begin)
+    int32_t* r_node_idx = nullptr;// [m]    in-neighbours        (gm_graph::r_node_idx)
+    bool owns = true;
+};
+
+// Device counters block (one allocation, mirrored to pinned host memory).
+enum {
+    CTR_COUNT = 0,       // generic per-launch counter (trimmed, visited, ...)
+    CTR_COUNT2,
+    CTR_COUNT3,
+    CTR_QLEN,            // length of the produced queue
+    CTR_QLEN2,
+    CTR_NEXT_COLOR,      // colour allocator (last colour handed out)
+    CTR_OVERFLOW,        // trim cascade overflow length
+    CTR_CHANGED,         // label propagation change flag
+    CTR_ERROR,           // device-side error code (bounded waits, capacity)
+    CTR_ERROR_INFO,
+    CTR_NUM_CLASSES,
+    CTR_SPARE0,
+    CTR_SPARE1,
+    CTR_SPARE2,
+    CTR_SPARE3,
+    CTR_SPARE4,
+    CTR_MAX = 32
+};
+
+// device error codes written to CTR_ERROR
+#define SCC_DEVERR_QUEUE_OVERFLOW 1
+#define SCC_DEVERR_WAIT_LIMIT     2
+#define SCC_DEVERR_COLOR_OVERFLOW 3
+
+struct scc_state {
+    int device = 0;
+    int32_t n = 0;
+    cudaStream_t stream = nullptr;
+    int kernels = 0;                 // kernels launched (statistics)
+    int64_t traversal_steps = 0;
+
+    int32_t* color = nullptr;        // G_Color [n]
+    int32_t* scc = nullptr;          // G_SCC   [n]
+    int32_t* wcc = nullptr;          // G_WCC   [n]
+    int32_t* live = nullptr;         // compact trim targets [n]
+    int32_t live_count = 0;          // host mirror; -1 = not built (trim_targets.size()==0)
+    int32_t* live_tmp = nullptr;     // [n] scratch list
+    int32_t* qa = nullptr;           // [2n+64] traversal queue A
+    int32_t* qb = nullptr;           // [2n+64] traversal queue B
+    uint8_t* mark = nullptr;         // [n rounded to 4] reachability marks (bit0 FW, bit1 BW)
+    int32_t* aux = nullptr;          // [n] per-vertex scratch (trim2 mates, pivot slots...)
+    int32_t* block_sums = nullptr;   // scan scratch
+    int32_t* ctr = nullptr;          // device counters [CTR_MAX]
+    int32_t* h_ctr = nullptr;        // pinned host mirror [CTR_MAX]
+
+    // per-colour slot arrays (index = colour id), capacity colour_cap
+    int64_t colour_cap = 0;
+    unsigned long long* slot_key = nullptr;  // pivot key per colour
+    int32_t* slot_pivot = nullptr;           // pivot vertex per colour
+    int32_t* slot_fw = nullptr;              // new fw colour per colour
+    int32_t* slot_bw = nullptr;              // new bw colour per colour
+    int32_t* slot_count = nullptr;           // member count per colour
+
+    // work queue (my_work items): classes that still need resolving
+    std::vector<int32_t> wq_colors;
+    std::vector<int32_t> wq_counts;
+
+    // learned pivot model (optional)
+    void* pivot_model = nullptr;
+
+    cudaEvent_t ev[16];
+    bool events = false;
+};
+
+// ---------------------------------------------------------------- helpers (host)
+static inline unsigned scc_blocks(int64_t n, int threads = SCC_THREADS, int64_t cap = 148LL * 16) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (unsigned)b;
+}
+int scc_sync_counters(scc_state* s);   // D2H copy of ctr -> h_ctr and stream sync
+int scc_zero_counters(scc_state* s, int first, int count);
+int scc_check_device_error(scc_state* s);
+
+// phase implementations shared between translation units
+int scc_impl_compact_live(const scc_graph* g, scc_state* s, bool from_all);
+int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* trimmed);
+int scc_impl_trim2(const scc_graph* g, scc_state* s, int32_t* trimmed);
+int scc_impl_ensure_colour_cap(scc_state* s, int64_t need);
+int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int32_t forced_pivot,
+                      int32_t* scc_found, int32_t* active_classes);
+int scc_impl_wcc(const scc_graph* g, scc_state* s);
+int scc_impl_resolve_all(const scc_graph* g, scc_state* s);
+int scc_impl_get_live_host(scc_state* s, std::vector<int32_t>& out);
+int scc_impl_count_colour(scc_state* s, int32_t color, int32_t* count);
+int scc_impl_build_graph_from_device_edges(int32_t n, int64_t m, const int32_t* d_src,
+                                           const int32_t* d_dst, int flags, int device,
+                                           scc_graph** out);
+int scc_impl_transpose(scc_graph* g, cudaStream_t st);

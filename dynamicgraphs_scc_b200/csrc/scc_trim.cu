@@ -1,0 +1,353 @@
+// Trim1 and Trim2.
+//
+// Trim1 (trim_once_node, src/scc_trim1.cc:38-110): a vertex of colour c with
+// no out-neighbour or no in-neighbour of colour c (self-loops ignored) is a
+// singleton SCC: colour -2, scc = itself.  The reference repeats whole sweeps
+// (repeat_global_trim1, scc_trim1.cc:195-209); here one launch peels to the
+// fixpoint: a thread that trims x re-checks x's same-colour neighbours right
+// away (after a device-scope fence, reading colours from L2) and follows the
+// chain on a small per-thread stack; stack overflow and high-degree vertices
+// go to an overflow list that the next launch expands one warp per vertex.
+// Two threads that each trim one of w's last two live neighbours both fence
+// before re-checking w, so at least one sees both trims and peels w: the
+// fixpoint is exact.
+//
+// Trim2 (trim_2nd_new_main, src/scc_trim2_new.cc:45-78): {n,k}, n<k, where n's
+// only live out-neighbour (ignoring self-loops and repeats) is k and k's is n,
+// or the same on in-edges, is a 2-vertex SCC with scc = n.  Decisions are
+// taken on the colours before the pass (a find kernel, then an apply kernel).
+#include "scc_internal.cuh"
+
+#define TRIM_STACK 8
+#define TRIM_BIG_DEG 512
+
+__device__ __forceinline__ int32_t ld_cg(const int32_t* p) { return __ldcg(p); }
+
+// true if v has a neighbour w != v of colour c in (off, adj)
+__device__ __forceinline__ bool has_live_nbr(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                             const int32_t* color, int32_t v, int32_t c) {
+    int32_t b = __ldg(off + v), e = __ldg(off + v + 1);
+    for (int32_t k = b; k < e; ++k) {
+        int32_t w = __ldg(adj + k);
+        if (w != v && ld_cg(color + w) == c) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool trimmable(const scc_graph& g, const int32_t* color, int32_t v, int32_t c) {
+    return !has_live_nbr(g.begin, g.node_idx, color, v, c) || !has_live_nbr(g.r_begin, g.r_node_idx, color, v, c);
+}
+
+struct TrimArgs {
+    const int32_t* begin; const int32_t* node_idx; const int32_t* r_begin; const int32_t* r_node_idx;
+    int32_t* color; int32_t* scc;
+    int32_t* ovf; int32_t* ctr;
+};
+
+__device__ __forceinline__ scc_graph as_graph(const TrimArgs& a) {
+    scc_graph g;
+    g.begin = const_cast<int32_t*>(a.begin); g.node_idx = const_cast<int32_t*>(a.node_idx);
+    g.r_begin = const_cast<int32_t*>(a.r_begin); g.r_node_idx = const_cast<int32_t*>(a.r_node_idx);
+    return g;
+}
+
+__device__ __forceinline__ void push_overflow(const TrimArgs& a, int32_t x) {
+    int32_t pos = atomicAdd(a.ctr + CTR_OVERFLOW, 1);
+    a.ovf[pos] = x;   // each vertex is trimmed once, so the list never exceeds n
+}
+
+// Try to trim w (colour c); on success record it.
+__device__ __forceinline__ bool try_trim(const TrimArgs& a, const scc_graph& g, int32_t w, int32_t c) {
+    if (ld_cg(a.color + w) != c) return false;
+    if (!trimmable(g, a.color, w, c)) return false;
+    if (atomicCAS(a.color + w, c, SCC_COLOR_DONE) != c) return false;
+    a.scc[w] = w;
+    __threadfence();
+    return true;
+}
+
+// Re-check the same-colour neighbours of trimmed x, following chains on a local stack.
+__device__ void cascade(const TrimArgs& a, const scc_graph& g, int32_t x0, int32_t c, int32_t& cnt) {
+    int32_t stk[TRIM_STACK];
+    int sp = 0;
+    stk[sp++] = x0;
+    while (sp > 0) {
+        int32_t x = stk[--sp];
+        int32_t d = (__ldg(a.begin + x + 1) - __ldg(a.begin + x)) + (__ldg(a.r_begin + x + 1) - __ldg(a.r_begin + x));
+        if (d > TRIM_BIG_DEG) { push_overflow(a, x); continue; }
+        for (int pass = 0; pass < 2; ++pass) {
+            const int32_t* off = pass ? a.r_begin : a.begin;
+            const int32_t* adj = pass ? a.r_node_idx : a.node_idx;
+            int32_t b = __ldg(off + x), e = __ldg(off + x + 1);
+            for (int32_t k = b; k < e; ++k) {
+                int32_t w = __ldg(adj + k);
+                if (w == x) continue;
+                if (try_trim(a, g, w, c)) {
+                    cnt++;
+                    if (sp < TRIM_STACK) stk[sp++] = w;
+                    else push_overflow(a, w);
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void block_count_add(int32_t* dst, int32_t v) {
+    v += __shfl_down_sync(0xFFFFFFFFu, v, 16);
+    v += __shfl_down_sync(0xFFFFFFFFu, v, 8);
+    v += __shfl_down_sync(0xFFFFFFFFu, v, 4);
+    v += __shfl_down_sync(0xFFFFFFFFu, v, 2);
+    v += __shfl_down_sync(0xFFFFFFFFu, v, 1);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
+}
+
+// Sweep: candidates are list[i] (or i when list == nullptr).
+__global__ void k_trim1_sweep(TrimArgs a, const int32_t* __restrict__ list, int64_t n_items) {
+    scc_graph g = as_graph(a);
+    int32_t cnt = 0;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t limit = ((n_items + 31) / 32) * 32;   // keep whole warps for the final reduction
+    for (int64_t i = start; i < limit; i += stride) {
+        if (i < n_items) {
+            int32_t v = list ? list[i] : (int32_t)i;
+            int32_t c = ld_cg(a.color + v);
+            if (c != SCC_COLOR_DONE && try_trim(a, g, v, c)) {
+                cnt++;
+                cascade(a, g, v, c, cnt);
+            }
+        }
+    }
+    block_count_add(a.ctr + CTR_COUNT, cnt);
+}
+
+// Overflow expansion: one warp per already-trimmed vertex x, lanes stride its
+// neighbours; newly trimmed neighbours cascade per lane.
+__global__ void k_trim1_overflow(TrimArgs a, const int32_t* __restrict__ items, int32_t n_items,
+                                 const int32_t* __restrict__ item_colors) {
+    scc_graph g = as_graph(a);
+    int lane = threadIdx.x & 31;
+    int32_t cnt = 0;
+    int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t wi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; wi < n_items; wi += wstride) {
+        int32_t x = items[wi];
+        int32_t c = item_colors[wi];
+        for (int pass = 0; pass < 2; ++pass) {
+            const int32_t* off = pass ? a.r_begin : a.begin;
+            const int32_t* adj = pass ? a.r_node_idx : a.node_idx;
+            int32_t b = __ldg(off + x), e = __ldg(off + x + 1);
+            for (int32_t k = b + lane; k < e; k += 32) {
+                int32_t w = __ldg(adj + k);
+                if (w != x && try_trim(a, g, w, c)) { cnt++; cascade(a, g, w, c, cnt); }
+            }
+        }
+    }
+    block_count_add(a.ctr + CTR_COUNT, cnt);
+}
+
+// The colour a trimmed vertex had is needed to re-check its neighbours; it is
+// recovered from any live neighbour?  No: the overflow list stores vertices
+// already set to -2, so their old colour is saved alongside by this kernel.
+__global__ void k_save_colors(const int32_t* __restrict__ items, int32_t n, const int32_t* __restrict__ saved_src,
+                              int32_t* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = saved_src[items[i]];
+}
+
+// Colour snapshot used to recover the colour a vertex had before it was trimmed.
+__global__ void k_copy_i32(int64_t n, const int32_t* __restrict__ a, int32_t* __restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = a[i];
+}
+__global__ void k_copy_list_i32(const int32_t* __restrict__ list, int64_t n, const int32_t* __restrict__ a,
+                                int32_t* __restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t v = list[i];
+        b[v] = a[v];
+    }
+}
+
+// Peel to the fixpoint over the live list (use_live) or all vertices.
+int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* trimmed) {
+    int64_t n_items = use_live ? s->live_count : g->n;
+    const int32_t* list = use_live ? s->live : nullptr;
+    *trimmed = 0;
+    if (n_items <= 0) return SCC_OK;
+    // snapshot colours (aux) so overflowed vertices keep their pre-trim colour
+    if (use_live)
+        k_copy_list_i32<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(list, n_items, s->color, s->aux);
+    else
+        k_copy_i32<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(n_items, s->color, s->aux);
+    SCC_LAUNCHED(s);
+    TrimArgs a;
+    a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin; a.r_node_idx = g->r_node_idx;
+    a.color = s->color; a.scc = s->scc; a.ctr = s->ctr;
+    a.ovf = s->qa;
+    SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
+    SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
+    k_trim1_sweep<<<scc_blocks(n_items, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, list, n_items);
+    SCC_LAUNCHED(s);
+    int64_t total = 0;
+    for (int round = 0; round < 1000000; ++round) {
+        SCC_TRY(scc_sync_counters(s));
+        total += s->h_ctr[CTR_COUNT];
+        int32_t novf = s->h_ctr[CTR_OVERFLOW];
+        if (novf == 0) break;
+        // expand overflowed vertices: move list qa -> qb, colours of items into live_tmp
+        SCC_CUDA(cudaMemcpyAsync(s->qb, s->qa, sizeof(int32_t) * (size_t)novf, cudaMemcpyDeviceToDevice, s->stream));
+        k_save_colors<<<scc_blocks(novf), SCC_THREADS, 0, s->stream>>>(s->qb, novf, s->aux, s->live_tmp);
+        SCC_LAUNCHED(s);
+        SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
+        SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
+        k_trim1_overflow<<<scc_blocks((int64_t)novf * 32, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(
+            a, s->qb, novf, s->live_tmp);
+        SCC_LAUNCHED(s);
+    }
+    *trimmed = (int32_t)total;
+    return SCC_OK;
+}
+
+// ------------------------------------------------------------------ trim2
+__device__ __forceinline__ bool degree_is_one(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                              const int32_t* __restrict__ color, int32_t c, int32_t v, int32_t* nbr) {
+    int32_t the = SCC_NIL_NODE;
+    int cnt = 0;
+    int32_t b = __ldg(off + v), e = __ldg(off + v + 1);
+    for (int32_t k = b; k < e; ++k) {
+        int32_t w = __ldg(adj + k);
+        if (w == v || w == the) continue;   // self edge, repeated edge
+        if (color[w] != c) continue;
+        cnt++;
+        the = w;
+        if (cnt == 2) return false;
+    }
+    *nbr = the;
+    return cnt == 1;
+}
+
+__global__ void k_trim2_find(const int32_t* __restrict__ begin, const int32_t* __restrict__ node_idx,
+                             const int32_t* __restrict__ r_begin, const int32_t* __restrict__ r_node_idx,
+                             const int32_t* __restrict__ color, const int32_t* __restrict__ list, int64_t n_items,
+                             int32_t* __restrict__ mate) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_items; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t n = list ? list[i] : (int32_t)i;
+        int32_t c = color[n];
+        int32_t res = SCC_NIL_NODE;
+        if (c != SCC_COLOR_DONE) {
+            int32_t k, kk;
+            if (degree_is_one(begin, node_idx, color, c, n, &k) && n < k &&
+                degree_is_one(begin, node_idx, color, c, k, &kk) && kk == n)
+                res = k;
+            else if (degree_is_one(r_begin, r_node_idx, color, c, n, &k) && n < k &&
+                     degree_is_one(r_begin, r_node_idx, color, c, k, &kk) && kk == n)
+                res = k;
+        }
+        mate[n] = res;
+    }
+}
+
+__global__ void k_trim2_apply(int32_t* __restrict__ color, int32_t* __restrict__ scc, const int32_t* __restrict__ list,
+                              int64_t n_items, const int32_t* __restrict__ mate, int32_t* __restrict__ count) {
+    int32_t cnt = 0;
+    int64_t limit = ((n_items + 31) / 32) * 32;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i < n_items) {
+            int32_t n = list ? list[i] : (int32_t)i;
+            int32_t k = (color[n] != SCC_COLOR_DONE) ? mate[n] : SCC_NIL_NODE;
+            if (k >= 0) {
+                color[n] = SCC_COLOR_DONE; color[k] = SCC_COLOR_DONE;
+                scc[n] = n; scc[k] = n;
+                cnt += 2;
+            }
+        }
+    }
+    block_count_add(count, cnt);
+}
+
+int scc_impl_trim2(const scc_graph* g, scc_state* s, int32_t* trimmed) {
+    *trimmed = 0;
+    bool use_live = s->live_count >= 0;
+    int64_t n_items = use_live ? s->live_count : g->n;
+    const int32_t* list = use_live ? s->live : nullptr;
+    if (n_items <= 0) return SCC_OK;
+    SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
+    k_trim2_find<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(g->begin, g->node_idx, g->r_begin, g->r_node_idx,
+                                                                    s->color, list, n_items, s->aux);
+    SCC_LAUNCHED(s);
+    k_trim2_apply<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(s->color, s->scc, list, n_items, s->aux,
+                                                                     s->ctr + CTR_COUNT);
+    SCC_LAUNCHED(s);
+    SCC_TRY(scc_sync_counters(s));
+    *trimmed = s->h_ctr[CTR_COUNT];
+    return SCC_OK;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" int scc_do_global_trim1(const scc_graph* g, scc_state* s, int32_t* trimmed) {
+    SCC_REQUIRE(g && s, SCC_ERR_INVALID, "NULL argument");
+    SCC_CUDA(cudaSetDevice(s->device));
+    int32_t t = 0;
+    SCC_TRY(scc_impl_trim1(g, s, false, &t));
+    if (trimmed) *trimmed = t;
+    return SCC_OK;
+}
+
+extern "C" int scc_do_global_trim1_compact(const scc_graph* g, scc_state* s, int32_t* trimmed) {
+    SCC_REQUIRE(g && s, SCC_ERR_INVALID, "NULL argument");
+    SCC_CUDA(cudaSetDevice(s->device));
+    int32_t t = 0;
+    SCC_TRY(scc_impl_trim1(g, s, s->live_count >= 0, &t));
+    if (trimmed) *trimmed = t;
+    return SCC_OK;
+}
+
+extern "C" int scc_repeat_global_trim1(const scc_graph* g, scc_state* s, int32_t trim_stop, int32_t* trimmed) {
+    SCC_REQUIRE(g && s, SCC_ERR_INVALID, "NULL argument");
+    (void)trim_stop;
+    SCC_CUDA(cudaSetDevice(s->device));
+    int32_t t = 0;
+    SCC_TRY(scc_impl_trim1(g, s, false, &t));
+    // scc_trim1.cc:203-205: once >= 10% are trimmed the reference continues on
+    // the compact list, which leaves trim_targets built.
+    if ((double)t >= (double)g->n * 0.1 && g->n > 0) SCC_TRY(scc_impl_compact_live(g, s, s->live_count < 0));
+    if (trimmed) *trimmed = t;
+    return SCC_OK;
+}
+
+extern "C" int scc_repeat_global_trim1_compact(const scc_graph* g, scc_state* s, int32_t trim_stop, int32_t* trimmed) {
+    SCC_REQUIRE(g && s, SCC_ERR_INVALID, "NULL argument");
+    (void)trim_stop;
+    SCC_CUDA(cudaSetDevice(s->device));
+    SCC_TRY(scc_impl_compact_live(g, s, false));
+    int32_t t = 0;
+    SCC_TRY(scc_impl_trim1(g, s, true, &t));
+    if (trimmed) *trimmed = t;
+    return SCC_OK;
+}
+
+extern "C" int scc_do_global_trim2_new(const scc_graph* g, scc_state* s, int32_t* trimmed) {
+    SCC_REQUIRE(g && s, SCC_ERR_INVALID, "NULL argument");
+    SCC_CUDA(cudaSetDevice(s->device));
+    int32_t t = 0;
+    SCC_TRY(scc_impl_trim2(g, s, &t));
+    if (trimmed) *trimmed = t;
+    return SCC_OK;
+}
+
+extern "C" int scc_do_global_trim2(const scc_graph* g, scc_state* s, int32_t* trimmed) {
+    return scc_do_global_trim2_new(g, s, trimmed);
+}
+
+extern "C" int scc_repeat_global_trim2_new(const scc_graph* g, scc_state* s, int32_t exit_count, int32_t* trimmed) {
+    SCC_REQUIRE(g && s, SCC_ERR_INVALID, "NULL argument");
+    SCC_CUDA(cudaSetDevice(s->device));
+    int64_t total = 0;
+    for (;;) {
+        int32_t t = 0;
+        SCC_TRY(scc_impl_trim2(g, s, &t));
+        total += t;
+        if (t <= exit_count || t == 0) break;
+    }
+    if (trimmed) *trimmed = (int32_t)total;
+    return SCC_OK;
+}

@@ -1,0 +1,340 @@
+"""Python mirror of the reference's SCC phase API over the C ABI.
+
+Names and argument meanings follow the reference's phase functions
+(ShashwaTTrigunayaT/DynamicGraphs_SCC src/scc.h:18-92): a ``Graph`` stands for
+gm_graph (int32 CSR + transpose, here resident on the GPU) and a ``State`` for
+the G_Color / G_SCC globals plus the work queue.  Errors raise ``SccError``
+instead of the reference's assert()/exit(1).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .capi import SccError, call, i32p
+
+METHOD_BASELINE = 0
+METHOD_GLOBAL_FB = 1
+METHOD_GLOBAL_WCC_FB = 2
+PIVOT_DEGREE = 0
+PIVOT_LEARNED = 1
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+
+
+class Graph:
+    """Device-resident CSR + transpose (gm_graph / GPUGraph)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+
+    # -- construction -------------------------------------------------------------------------
+    @classmethod
+    def from_edges(cls, n: int, src, dst, flags: int = capi.SCC_BUILD_KEEP_ALL, device: int = 0) -> "Graph":
+        s, d = _i32(src), _i32(dst)
+        if s.shape != d.shape:
+            raise ValueError("src and dst differ in length")
+        h = C.c_void_p()
+        call("scc_graph_create_edges", n, int(s.size), i32p(s), i32p(d), flags, device, C.byref(h))
+        return cls(h)
+
+    @classmethod
+    def from_csr(cls, begin, node_idx, r_begin=None, r_node_idx=None, device: int = 0) -> "Graph":
+        b, a = _i32(begin), _i32(node_idx)
+        rb = _i32(r_begin) if r_begin is not None else None
+        ra = _i32(r_node_idx) if r_node_idx is not None else None
+        h = C.c_void_p()
+        call("scc_graph_create_csr", int(b.size - 1), int(a.size), i32p(b), i32p(a), i32p(rb), i32p(ra), device,
+             C.byref(h))
+        return cls(h)
+
+    @classmethod
+    def load_edge_list(cls, path: str, device: int = 0) -> "Graph":
+        h = C.c_void_p()
+        call("scc_graph_load_edge_list", path.encode(), device, C.byref(h))
+        return cls(h)
+
+    @classmethod
+    def load_binary(cls, path: str, device: int = 0) -> "Graph":
+        h = C.c_void_p()
+        call("scc_graph_load_binary", path.encode(), device, C.byref(h))
+        return cls(h)
+
+    @classmethod
+    def generate(cls, rmat_scale=0, edge_factor=0, grid_side=0, num_cycles=0, cycle_min=3, cycle_max=100000,
+                 seed=1, flags=capi.SCC_BUILD_DEDUP | capi.SCC_BUILD_NO_SELF_LOOPS, device=0) -> "Graph":
+        p = gen_params(rmat_scale, edge_factor, grid_side, num_cycles, cycle_min, cycle_max, seed)
+        h = C.c_void_p()
+        call("scc_gen_graph", C.byref(p), flags, device, C.byref(h))
+        return cls(h)
+
+    # -- properties ---------------------------------------------------------------------------
+    @property
+    def handle(self) -> C.c_void_p:
+        if self._h is None:
+            raise SccError(5, "Graph", "graph was freed")
+        return self._h
+
+    def num_nodes(self) -> int:
+        n = C.c_int32()
+        call("scc_graph_num_nodes", self.handle, C.byref(n))
+        return n.value
+
+    def num_edges(self) -> int:
+        m = C.c_int64()
+        call("scc_graph_num_edges", self.handle, C.byref(m))
+        return m.value
+
+    def csr(self):
+        n, m = self.num_nodes(), self.num_edges()
+        b = np.empty(n + 1, np.int32); a = np.empty(m, np.int32)
+        rb = np.empty(n + 1, np.int32); ra = np.empty(m, np.int32)
+        call("scc_graph_copy_csr", self.handle, i32p(b), i32p(a), i32p(rb), i32p(ra))
+        return b, a, rb, ra
+
+    def save_binary(self, path: str) -> None:
+        call("scc_graph_save_binary", self.handle, path.encode())
+
+    def free(self) -> None:
+        if self._h is not None:
+            capi.lib().scc_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def gen_params(rmat_scale=0, edge_factor=0, grid_side=0, num_cycles=0, cycle_min=3, cycle_max=100000, seed=1):
+    return capi.GenParams(rmat_scale, edge_factor, grid_side, num_cycles, cycle_min, cycle_max, seed)
+
+
+def generate_edges_host(**kw):
+    """Raw seeded edge list on the host (the same multiset Graph.generate builds)."""
+    p = gen_params(**kw)
+    n = C.c_int32(); cap = C.c_int64()
+    call("scc_gen_sizes", C.byref(p), C.byref(n), C.byref(cap))
+    src = np.empty(max(cap.value, 1), np.int32)
+    dst = np.empty(max(cap.value, 1), np.int32)
+    m = C.c_int64()
+    call("scc_gen_edges_host", C.byref(p), i32p(src), i32p(dst), cap.value, C.byref(m))
+    return n.value, src[:m.value], dst[:m.value]
+
+
+class State:
+    """G_Color / G_SCC / work queue (GPUState); one per graph run."""
+
+    def __init__(self, graph: Graph):
+        self.graph = graph
+        h = C.c_void_p()
+        call("scc_state_create", graph.handle, C.byref(h))
+        self._h = h
+        self.n = graph.num_nodes()
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise SccError(5, "State", "state was freed")
+        return self._h
+
+    def _g(self):
+        return self.graph.handle
+
+    def _out(self):
+        return C.c_int32(0)
+
+    # -- arrays ----------------------------------------------------------------------------------
+    def reset(self):
+        call("scc_state_reset", self.handle)
+
+    def color(self) -> np.ndarray:
+        a = np.empty(self.n, np.int32)
+        call("scc_state_get_color", self.handle, i32p(a))
+        return a
+
+    def scc(self) -> np.ndarray:
+        a = np.empty(self.n, np.int32)
+        call("scc_state_get_scc", self.handle, i32p(a))
+        return a
+
+    def wcc(self) -> np.ndarray:
+        a = np.empty(self.n, np.int32)
+        call("scc_state_get_wcc", self.handle, i32p(a))
+        return a
+
+    def set_color(self, a) -> None:
+        call("scc_state_set_color", self.handle, i32p(_i32(a)))
+
+    def set_scc(self, a) -> None:
+        call("scc_state_set_scc", self.handle, i32p(_i32(a)))
+
+    def trim_targets(self) -> np.ndarray:
+        c = C.c_int32()
+        call("scc_state_get_trim_targets", self.handle, None, 0, C.byref(c))
+        a = np.empty(c.value, np.int32)
+        call("scc_state_get_trim_targets", self.handle, i32p(a), c.value, C.byref(c))
+        return a
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        call("scc_state_stream", self.handle, C.byref(p))
+        return p.value or 0
+
+    def synchronize(self) -> None:
+        call("scc_state_synchronize", self.handle)
+
+    # -- colour ----------------------------------------------------------------------------------
+    def get_new_color(self) -> int:
+        o = self._out(); call("scc_get_new_color", self.handle, C.byref(o)); return o.value
+
+    def get_curr_color(self) -> int:
+        o = self._out(); call("scc_get_curr_color", self.handle, C.byref(o)); return o.value
+
+    def choose_pivot_from_color(self, color: int) -> int:
+        o = self._out()
+        rc = capi.lib().scc_choose_pivot_from_color(self._g(), self.handle, color, C.byref(o))
+        if rc == 7:
+            return capi.SCC_NIL_NODE
+        if rc != 0:
+            raise SccError(rc, "scc_choose_pivot_from_color", capi.lib().scc_last_error().decode())
+        return o.value
+
+    def generate_compact_set(self, color: int) -> np.ndarray:
+        c = C.c_int32()
+        call("scc_generate_compact_set", self._g(), self.handle, color, None, 0, C.byref(c))
+        a = np.empty(c.value, np.int32)
+        call("scc_generate_compact_set", self._g(), self.handle, color, i32p(a), c.value, C.byref(c))
+        return a
+
+    # -- trim ------------------------------------------------------------------------------------
+    def do_global_trim1(self) -> int:
+        o = self._out(); call("scc_do_global_trim1", self._g(), self.handle, C.byref(o)); return o.value
+
+    def do_global_trim1_compact(self) -> int:
+        o = self._out(); call("scc_do_global_trim1_compact", self._g(), self.handle, C.byref(o)); return o.value
+
+    def repeat_global_trim1(self, trim_stop: int = 100) -> int:
+        o = self._out(); call("scc_repeat_global_trim1", self._g(), self.handle, trim_stop, C.byref(o)); return o.value
+
+    def repeat_global_trim1_compact(self, trim_stop: int = 100) -> int:
+        o = self._out()
+        call("scc_repeat_global_trim1_compact", self._g(), self.handle, trim_stop, C.byref(o))
+        return o.value
+
+    def create_trim1_compact(self) -> int:
+        o = self._out(); call("scc_create_trim1_compact", self._g(), self.handle, C.byref(o)); return o.value
+
+    def do_global_trim2_new(self) -> int:
+        o = self._out(); call("scc_do_global_trim2_new", self._g(), self.handle, C.byref(o)); return o.value
+
+    def do_global_trim2(self) -> int:
+        o = self._out(); call("scc_do_global_trim2", self._g(), self.handle, C.byref(o)); return o.value
+
+    def repeat_global_trim2_new(self, exit_count: int = 100) -> int:
+        o = self._out()
+        call("scc_repeat_global_trim2_new", self._g(), self.handle, exit_count, C.byref(o))
+        return o.value
+
+    # -- FW-BW / WCC ---------------------------------------------------------------------------
+    def do_fw_bw_global_main(self, curr_color: int = -1, count: int = 0, create_work_items: bool = False) -> int:
+        o = self._out()
+        call("scc_do_fw_bw_global_main", self._g(), self.handle, curr_color, count, int(create_work_items), C.byref(o))
+        return o.value
+
+    def do_fw_bw_global_pivot(self, curr_color: int, pivot: int, create_work_items: bool = False) -> int:
+        o = self._out()
+        call("scc_do_fw_bw_global_pivot", self._g(), self.handle, curr_color, pivot, int(create_work_items), C.byref(o))
+        return o.value
+
+    def create_works_after_bfs_trim(self) -> int:
+        o = self._out(); call("scc_create_works_after_bfs_trim", self._g(), self.handle, C.byref(o)); return o.value
+
+    def start_workers_fw_bw(self, local_items: int = 1) -> None:
+        call("scc_start_workers_fw_bw", self._g(), self.handle, local_items)
+
+    def start_workers_fw_bw_dfs(self, local_items: int = 40) -> None:
+        call("scc_start_workers_fw_bw_dfs", self._g(), self.handle, local_items)
+
+    def work_q_size(self) -> int:
+        o = self._out(); call("scc_work_q_size", self.handle, C.byref(o)); return o.value
+
+    def work_q_items(self):
+        k = C.c_int32()
+        call("scc_work_q_items", self.handle, None, None, 0, C.byref(k))
+        cols = np.empty(k.value, np.int32); cnts = np.empty(k.value, np.int32)
+        call("scc_work_q_items", self.handle, i32p(cols), i32p(cnts), k.value, C.byref(k))
+        return cols, cnts
+
+    def do_global_wcc(self) -> None:
+        call("scc_do_global_wcc", self._g(), self.handle)
+
+    def create_work_items_from_wcc(self) -> int:
+        o = self._out(); call("scc_create_work_items_from_wcc", self._g(), self.handle, C.byref(o)); return o.value
+
+    # -- driver ----------------------------------------------------------------------------------
+    def run(self, method: int = METHOD_GLOBAL_WCC_FB, pivot_mode: int = PIVOT_DEGREE) -> dict:
+        st = capi.RunStats()
+        call("scc_run", self._g(), self.handle, method, pivot_mode, C.byref(st))
+        return st.as_dict()
+
+    def count_sccs(self) -> int:
+        o = self._out(); call("scc_count_sccs", self.handle, C.byref(o)); return o.value
+
+    def canonical_labels(self) -> np.ndarray:
+        a = np.empty(self.n, np.int32)
+        call("scc_canonical_labels", self.handle, i32p(a))
+        return a
+
+    def output_scc_list(self, path: str = "scc_list.txt") -> None:
+        call("scc_output_scc_list", self.handle, path.encode())
+
+    def histogram(self):
+        k = C.c_int32()
+        call("scc_histogram", self.handle, None, None, 0, C.byref(k))
+        sz = np.empty(k.value, np.int32); ct = np.empty(k.value, np.int32)
+        call("scc_histogram", self.handle, i32p(sz), i32p(ct), k.value, C.byref(k))
+        return dict(zip(sz.tolist(), ct.tolist()))
+
+    def free(self) -> None:
+        if self._h is not None:
+            capi.lib().scc_state_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def read_scc_list(path: str, n: int):
+    a = np.empty(n, np.int32)
+    k = C.c_int32()
+    call("scc_read_scc_list", path.encode(), n, i32p(a), C.byref(k))
+    return a, k.value
+
+
+def decompose_csr(begin, node_idx, r_begin=None, r_node_idx=None, method: int = METHOD_GLOBAL_WCC_FB, device=0):
+    """Host CSR in, canonical labels out (H2D + run + D2H in one call)."""
+    b, a = _i32(begin), _i32(node_idx)
+    rb = _i32(r_begin) if r_begin is not None else None
+    ra = _i32(r_node_idx) if r_node_idx is not None else None
+    n = b.size - 1
+    labels = np.empty(n, np.int32)
+    k = C.c_int32()
+    st = capi.RunStats()
+    call("scc_decompose_csr", n, int(a.size), i32p(b), i32p(a), i32p(rb), i32p(ra), method, device, i32p(labels),
+         C.byref(k), C.byref(st))
+    return labels, k.value, st.as_dict()
+
+
+def device_count() -> int:
+    c = C.c_int()
+    call("scc_device_count", C.byref(c))
+    return c.value

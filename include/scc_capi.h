@@ -1,0 +1,243 @@
+/*
+ * scc_capi.h -- C ABI of the B200 strongly-connected-components engine.
+ *
+ * Drop-in boundary for the SCC path of ShashwaTTrigunayaT/DynamicGraphs_SCC.
+ * The reference exposes that path as a global-state C++ phase API
+ * (src/scc.h:18-92) over gm_graph's int32 CSR (gm_graph/inc/gm_graph.h) and as
+ * a CUDA host API over GPUGraph/GPUState (src_CUDA/scc_cuda.h:26-490).  This
+ * header replaces both with opaque handles and plain pointers:
+ *
+ *   gm_graph / GPUGraph       -> scc_graph  (device CSR + transpose, int32)
+ *   G_Color, G_SCC / GPUState -> scc_state  (device colour / SCC arrays + work space)
+ *   global work queue         -> device-resident colour classes inside scc_state
+ *
+ * Every entry point returns an int status (SCC_OK == 0) instead of the
+ * reference's assert()/exit(1) (src_CUDA/scc_cuda.h:61-67); counts come back
+ * through out-parameters.  scc_last_error() describes the last failure on the
+ * calling thread.  All arrays are int32 (gm_graph/inc/gm_graph_typedef.h:17-20).
+ *
+ * Colours follow the reference (src/scc.h:19-22): -1 initial, -2 SCC found,
+ * fresh colours >= 0 from scc_get_new_color().  scc[v] is the representative
+ * vertex of v's SCC (G_SCC); scc_canonical_labels() turns it into the
+ * smallest member id of the component.
+ *
+ * Threading: one handle may be used by one host thread at a time; work on a
+ * state is ordered on the state's CUDA stream.  Host pointers may be pageable
+ * or pinned; "_device" variants take device pointers.
+ */
+#ifndef SCC_CAPI_H
+#define SCC_CAPI_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------------- */
+#define SCC_OK               0
+#define SCC_ERR_INVALID      1   /* bad argument (null handle, negative size, id out of range) */
+#define SCC_ERR_CUDA         2   /* CUDA runtime error (message in scc_last_error) */
+#define SCC_ERR_OOM          3   /* device allocation failed or budget exceeded */
+#define SCC_ERR_TIMEOUT      4   /* a bounded device wait gave up; the state is still usable after scc_state_reset */
+#define SCC_ERR_STATE        5   /* call out of order (e.g. phase before scc_state_create) */
+#define SCC_ERR_IO           6   /* file could not be read or written */
+#define SCC_ERR_NOT_FOUND    7   /* no vertex of the requested colour (NIL_NODE in the reference) */
+#define SCC_ERR_UNSUPPORTED  8   /* method or flag not offered by this engine */
+
+#define SCC_NIL_NODE (-1)        /* gm_graph::NIL_NODE */
+#define SCC_COLOR_INIT (-1)
+#define SCC_COLOR_DONE (-2)
+
+typedef struct scc_graph scc_graph;
+typedef struct scc_state scc_state;
+
+const char* scc_status_string(int status);
+const char* scc_last_error(void);
+int scc_version(void);                       /* major*10000 + minor*100 + patch */
+int scc_device_count(int* count);
+
+/* ---- graph (gm_graph / GPUGraph) ---------------------------------------------------- */
+/* Build flags for scc_graph_create_edges*. */
+#define SCC_BUILD_KEEP_ALL      0   /* keep duplicates and self-loops (gm_graph semantics) */
+#define SCC_BUILD_DEDUP         1   /* drop duplicate edges */
+#define SCC_BUILD_NO_SELF_LOOPS 2   /* drop self-loops */
+
+/* Edge list -> sorted CSR + sorted transpose on the device.  Replaces gm_graph
+ * add_node()/add_edge() + freeze() + do_semi_sort() + make_reverse_edges()
+ * (gm_graph/src/gm_graph.cc:459-480, 60-101, 385-420, 193-287) and
+ * graph_upload() (src_CUDA/scc_cuda_graph.cu:4).  Ids must be in [0, n). */
+int scc_graph_create_edges(int32_t n, int64_t m, const int32_t* src, const int32_t* dst,
+                           int flags, int device, scc_graph** out);
+int scc_graph_create_edges_device(int32_t n, int64_t m, const int32_t* d_src, const int32_t* d_dst,
+                                  int flags, int device, scc_graph** out);
+/* CSR (+ optional transpose; NULL r_begin/r_node_idx = build it on the device).
+ * Mirrors graph_upload(GPUGraph&, h_begin, h_node_idx, h_r_begin, h_r_node_idx, N, M)
+ * (src_CUDA/scc_cuda.h:72-77).  Adjacency lists must be sorted (gm_graph keeps them
+ * semi-sorted); the engine does not re-sort a caller's CSR. */
+int scc_graph_create_csr(int32_t n, int32_t m, const int32_t* begin, const int32_t* node_idx,
+                         const int32_t* r_begin, const int32_t* r_node_idx, int device, scc_graph** out);
+int scc_graph_create_csr_device(int32_t n, int32_t m, const int32_t* d_begin, const int32_t* d_node_idx,
+                                const int32_t* d_r_begin, const int32_t* d_r_node_idx, int device,
+                                scc_graph** out);
+/* Text edge list "u v" per line, 1-based, N = max id (src/common_main.h:61-83,
+ * the fast parser of src_CUDA/scc_cuda_dynamic.cpp:59-147).  Lines starting
+ * with '%' or '#' are skipped.  Duplicates and self-loops are kept. */
+int scc_graph_load_edge_list(const char* path, int device, scc_graph** out);
+/* Re-upload host CSR arrays into an existing graph of the same n and m (no
+ * allocation): the per-request H2D of graph_upload (src_CUDA/scc_cuda_graph.cu:4)
+ * for callers that keep the device graph between runs.  Ordered on `stream`
+ * (cudaStream_t as void*, NULL = legacy default stream). */
+int scc_graph_upload_csr(scc_graph* g, const int32_t* begin, const int32_t* node_idx,
+                         const int32_t* r_begin, const int32_t* r_node_idx, void* stream);
+int scc_graph_free(scc_graph* g);                             /* graph_free() */
+int scc_graph_num_nodes(const scc_graph* g, int32_t* n);
+int scc_graph_num_edges(const scc_graph* g, int64_t* m);
+/* Copy the CSR and transpose back to host arrays (n+1, m, n+1, m ints; any may be NULL). */
+int scc_graph_copy_csr(const scc_graph* g, int32_t* begin, int32_t* node_idx,
+                       int32_t* r_begin, int32_t* r_node_idx);
+/* Device pointers of the CSR arrays (borrowed; valid until scc_graph_free). */
+int scc_graph_device_csr(const scc_graph* g, const int32_t** d_begin, const int32_t** d_node_idx,
+                         const int32_t** d_r_begin, const int32_t** d_r_node_idx);
+/* Binary CSR snapshot (own format, little-endian: magic "SCCCSR01", n, m, begin, node_idx). */
+int scc_graph_save_binary(const scc_graph* g, const char* path);
+int scc_graph_load_binary(const char* path, int device, scc_graph** out);
+
+/* ---- state (G_Color / G_SCC / GPUState + phase globals) ------------------------------ */
+/* prepare() of src/scc_main.cc:96-118: G_SCC = NIL, colours = -1, colour
+ * counter reset, work queue empty, compact trim targets empty. */
+int scc_state_create(const scc_graph* g, scc_state** out);
+int scc_state_reset(scc_state* s);
+int scc_state_free(scc_state* s);
+int scc_state_synchronize(scc_state* s);
+/* The CUDA stream all work on this state is ordered on (cudaStream_t as void*). */
+int scc_state_stream(scc_state* s, void** stream);
+/* Host <-> device copies of G_Color / G_SCC (n ints each). */
+int scc_state_get_color(scc_state* s, int32_t* color);
+int scc_state_get_scc(scc_state* s, int32_t* scc);
+int scc_state_set_color(scc_state* s, const int32_t* color);
+int scc_state_set_scc(scc_state* s, const int32_t* scc);
+/* G_WCC labels (raw, with the 0x20000000 high-degree flag; -1 for finished vertices). */
+int scc_state_get_wcc(scc_state* s, int32_t* wcc);
+/* Compact trim targets (get_compact_trim_targets, src/scc_trim1.cc:32). */
+int scc_state_get_trim_targets(scc_state* s, int32_t* out, int32_t capacity, int32_t* count);
+int scc_state_device_arrays(scc_state* s, int32_t** d_color, int32_t** d_scc);
+
+/* ---- colour (src/scc_color.cc) --------------------------------------------------------- */
+int scc_get_new_color(scc_state* s, int32_t* color);          /* get_new_color,  scc_color.cc:38-54 */
+int scc_get_curr_color(scc_state* s, int32_t* color);         /* get_curr_color, scc_color.cc:56-61 */
+/* choose_pivot_from_color (scc_color.cc:64-93).  This engine's rule: the vertex
+ * of that colour with the largest in-degree x out-degree (ties: fixed id hash).
+ * SCC_ERR_NOT_FOUND and *pivot = SCC_NIL_NODE when the colour is empty. */
+int scc_choose_pivot_from_color(const scc_graph* g, scc_state* s, int32_t color, int32_t* pivot);
+/* generate_compact_set (scc_color.cc:95-113): members of a colour, ascending. */
+int scc_generate_compact_set(const scc_graph* g, scc_state* s, int32_t color,
+                             int32_t* out, int32_t capacity, int32_t* count);
+
+/* ---- trim1 (src/scc_trim1.cc) ---------------------------------------------------------- */
+/* One sweep: do_global_trim1 (scc_trim1.cc:112-135).  Trimmed vertices cascade
+ * inside the sweep; *trimmed counts them. */
+int scc_do_global_trim1(const scc_graph* g, scc_state* s, int32_t* trimmed);
+/* do_global_trim1_compact (scc_trim1.cc:137-163): same over the compact targets. */
+int scc_do_global_trim1_compact(const scc_graph* g, scc_state* s, int32_t* trimmed);
+/* repeat_global_trim1(G, TRIM_STOP) (scc_trim1.cc:195-209): sweeps until a
+ * sweep trims <= trim_stop vertices; this engine peels to the fixpoint whatever
+ * trim_stop is (the CUDA reference's TRIM_STOP=0), and also rebuilds the
+ * compact targets as the reference does once 10% are trimmed. */
+int scc_repeat_global_trim1(const scc_graph* g, scc_state* s, int32_t trim_stop, int32_t* trimmed);
+/* repeat_global_trim1_compact (scc_trim1.cc:277-290): create_trim1_compact + sweeps. */
+int scc_repeat_global_trim1_compact(const scc_graph* g, scc_state* s, int32_t trim_stop, int32_t* trimmed);
+/* create_trim1_compact (scc_trim1.cc:266-275): live vertices (colour != -2), ascending. */
+int scc_create_trim1_compact(const scc_graph* g, scc_state* s, int32_t* live_count);
+
+/* ---- trim2 (src/scc_trim2_new.cc, src/scc_trim2.cc) ---------------------------------- */
+/* do_global_trim2_new (scc_trim2_new.cc:80-102): 2-vertex SCCs among the compact
+ * targets, decided on the colours as they stood before the pass. */
+int scc_do_global_trim2_new(const scc_graph* g, scc_state* s, int32_t* trimmed);
+/* do_global_trim2 (scc_trim2.cc:24-152): same 2-SCC rule (alias). */
+int scc_do_global_trim2(const scc_graph* g, scc_state* s, int32_t* trimmed);
+/* repeat_global_trim2_new (scc_trim2_new.cc:105-114): until a pass trims <= exit_count. */
+int scc_repeat_global_trim2_new(const scc_graph* g, scc_state* s, int32_t exit_count, int32_t* trimmed);
+
+/* ---- FW-BW (src/scc_fb_global.cc, src/scc_fb_seq*.cc) ------------------------------- */
+/* do_fw_bw_global_main(G, curr_color, count, create_work_items) (scc_fb_global.cc:133-219).
+ * Pivot by scc_choose_pivot_from_color; FW set -> new colour, FW&BW -> SCC
+ * (scc = pivot), BW only -> second new colour, rest keeps curr_color.  Returns
+ * the SCC size.  count == 1 finishes the pivot alone, as the reference does. */
+int scc_do_fw_bw_global_main(const scc_graph* g, scc_state* s, int32_t curr_color, int32_t count,
+                             int create_work_items, int32_t* scc_size);
+/* Same with an explicit pivot (the met 6/11 good_init_pivot override, scc_fb_global.cc:140-147). */
+int scc_do_fw_bw_global_pivot(const scc_graph* g, scc_state* s, int32_t curr_color, int32_t pivot,
+                              int create_work_items, int32_t* scc_size);
+/* create_works_after_bfs_trim (scc_fb_global.cc:223-283): queue the fw/bw/base classes. */
+int scc_create_works_after_bfs_trim(const scc_graph* g, scc_state* s, int32_t* num_items);
+/* start_workers_fw_bw(G, N) (scc_fb_seq.cc:303-349) and start_workers_fw_bw_dfs(G, N)
+ * (scc_fb_seq2.cc:292-351): resolve every queued colour class to SCCs.  Here
+ * all classes advance together on the device (pivot per class, FW and BW
+ * reachability, split, trim) until none is left; local_items is accepted for
+ * interface parity. */
+int scc_start_workers_fw_bw(const scc_graph* g, scc_state* s, int32_t local_items);
+int scc_start_workers_fw_bw_dfs(const scc_graph* g, scc_state* s, int32_t local_items);
+int scc_work_q_size(scc_state* s, int32_t* size);            /* work_q_size, my_work_queue.cc */
+/* Work item table: colour and member count of each queued class (my_work{color,count}). */
+int scc_work_q_items(scc_state* s, int32_t* colors, int32_t* counts, int32_t capacity, int32_t* num_items);
+
+/* ---- WCC (src/scc_weak.cc) ------------------------------------------------------------ */
+/* do_global_wcc (scc_weak.cc:128-196): over the compact targets, label =
+ * minimum raw id (t, or t|0x20000000 when out-degree >= 50) over the same-colour
+ * vertices reachable from t; each root (label == itself) gets a new colour and
+ * its members take it. */
+int scc_do_global_wcc(const scc_graph* g, scc_state* s);
+/* create_work_items_from_wcc (scc_weak.cc:198-271): one queued class per root. */
+int scc_create_work_items_from_wcc(const scc_graph* g, scc_state* s, int32_t* num_items);
+
+/* ---- driver (src/scc_main.cc) ---------------------------------------------------------- */
+#define SCC_METHOD_BASELINE       0   /* Trim1 + FW-BW */
+#define SCC_METHOD_GLOBAL_FB      1   /* Trim1 + Global FW-BW + Trim1 + FW-BW */
+#define SCC_METHOD_GLOBAL_WCC_FB  2   /* Trim1 + Global FW-BW + Trim1/2 + WCC + FW-BW */
+
+#define SCC_PIVOT_DEGREE  0           /* max in-degree x out-degree */
+#define SCC_PIVOT_LEARNED 1           /* MLP-scored pivot (scc_pivot_model_* must be loaded) */
+
+typedef struct scc_run_stats {
+    double ms_total;                  /* device time of the run (CUDA events) */
+    double ms_trim1, ms_global_fb, ms_trim12, ms_wcc, ms_fb;   /* PHASE timers */
+    int32_t trimmed_first;            /* first repeat_global_trim1 */
+    int32_t first_scc_size;           /* do_fw_bw_global_main result */
+    int32_t trimmed_second;           /* trim1 + trim2 + trim1 after the global step */
+    int32_t num_sccs;                 /* "Total # SCCs" */
+    int32_t num_wcc_classes;          /* work items created from WCC */
+    int32_t fb_rounds;                /* device FW-BW rounds of the recursive phase */
+    int64_t traversal_steps;          /* reachability steps launched */
+    int32_t kernels_launched;         /* kernels this run launched */
+    int32_t pivot_mode;
+} scc_run_stats;
+
+/* my_main::run (src/scc_main.cc:120-145) for methods 0, 1, 2 (5-7 and 11 map
+ * to 2 as in check_args, scc_main.cc:170-171).  Method 3/4 (Tarjan) are the
+ * sequential oracle in the reference and are not offered here
+ * (SCC_ERR_UNSUPPORTED).  stats may be NULL. */
+int scc_run(const scc_graph* g, scc_state* s, int method, int pivot_mode, scc_run_stats* stats);
+/* post_process count (scc_main.cc:147-178): #v with scc[v] == v. */
+int scc_count_sccs(scc_state* s, int32_t* count);
+/* Canonical labels: smallest member id of each vertex's SCC (n ints). */
+int scc_canonical_labels(scc_state* s, int32_t* labels);
+int scc_canonical_labels_device(scc_state* s, int32_t* d_labels);
+/* output_scc_list (src/scc_post_analyze.cc:31-53): "i id" lines, ids numbered
+ * by first appearance.  path NULL = "scc_list.txt". */
+int scc_output_scc_list(scc_state* s, const char* path);
+/* read_file1 (src/common_main.h:316-341): labels from an scc_list.txt; *num_sccs = max id + 1. */
+int scc_read_scc_list(const char* path, int32_t n, int32_t* labels, int32_t* num_sccs);
+/* create_histogram_and_print (scc_post_analyze.cc:235-261): sizes[i], counts[i] ascending by size. */
+int scc_histogram(scc_state* s, int32_t* sizes, int32_t* counts, int32_t capacity, int32_t* num_bins);
+
+/* One-call convenience: host CSR in, canonical labels out (H2D + run + D2H). */
+int scc_decompose_csr(int32_t n, int32_t m, const int32_t* begin, const int32_t* node_idx,
+                      const int32_t* r_begin, const int32_t* r_node_idx, int method, int device,
+                      int32_t* labels, int32_t* num_sccs, scc_run_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCC_CAPI_H */

@@ -1,0 +1,168 @@
+"""CPU oracle for the SCC engine -- TEST INFRASTRUCTURE ONLY.
+
+Loads two native libraries built by oracle/Makefile:
+  build/liboracle.so  -- the C restatement of the reference algorithms (scc_oracle.c);
+  _ref/libscc_ref.so  -- the reference's own OpenMP engine compiled from its sources
+                         plus ref_harness.cc (optional: absent if never built).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libscc_ref.so")
+REF_CLI = os.path.join(HERE, "_ref", "scc")
+
+_I32P = C.POINTER(C.c_int32)
+_U8P = C.POINTER(C.c_uint8)
+_I64P = C.POINTER(C.c_int64)
+_lib = None
+_ref = None
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_I32P)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(ORACLE_SO)
+        L.orc_build_csr.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P, _I32P, _I32P, _I32P, _I32P]
+        L.orc_build_csr.restype = None
+        L.orc_tarjan.argtypes = [C.c_int32, _I32P, _I32P, _I32P]
+        L.orc_tarjan.restype = None
+        L.orc_canonical.argtypes = [C.c_int32, _I32P, _I32P]
+        L.orc_canonical.restype = None
+        L.orc_scc_canonical.argtypes = [C.c_int32, _I32P, _I32P, _I32P]
+        L.orc_scc_canonical.restype = None
+        L.orc_trim1_fixpoint.argtypes = [C.c_int32, _I32P, _I32P, _I32P, _I32P, _I32P, _I32P]
+        L.orc_trim1_fixpoint.restype = C.c_int64
+        L.orc_trim2.argtypes = [C.c_int32, _I32P, _I32P, _I32P, _I32P, _I32P, _I32P]
+        L.orc_trim2.restype = C.c_int64
+        L.orc_wcc_minreach.argtypes = [C.c_int32, _I32P, _I32P, _I32P, _I32P, _I32P]
+        L.orc_wcc_minreach.restype = None
+        L.orc_reach.argtypes = [C.c_int32, _I32P, _I32P, _I32P, C.c_int32, C.c_int32, _U8P]
+        L.orc_reach.restype = C.c_int64
+        L.orc_fw_bw.argtypes = [C.c_int32, _I32P, _I32P, _I32P, _I32P, _I32P, _I32P, C.c_int32, C.c_int32,
+                                C.c_int32, C.c_int32, _I64P, _I64P]
+        L.orc_fw_bw.restype = C.c_int64
+        L.orc_choose_pivot.argtypes = [C.c_int32, _I32P, _I32P, _I32P, C.c_int32]
+        L.orc_choose_pivot.restype = C.c_int32
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        L = C.CDLL(REF_SO)
+        L.ref_method2.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P, C.c_int, C.c_int, _I32P,
+                                  C.POINTER(C.c_double)]
+        L.ref_method2.restype = C.c_int
+        L.ref_tarjan.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P, _I32P, C.POINTER(C.c_double)]
+        L.ref_tarjan.restype = C.c_int
+        _ref = L
+    return _ref
+
+
+# ------------------------------------------------------------------------ graph helpers
+def dedup_edges(src, dst, drop_self_loops=True):
+    """Remove self-loops and duplicate (src, dst) pairs (the generators' post-processing)."""
+    s = np.asarray(src, np.int64)
+    d = np.asarray(dst, np.int64)
+    if drop_self_loops:
+        keep = s != d
+        s, d = s[keep], d[keep]
+    key = np.unique((s << 32) | d)
+    return (key >> 32).astype(np.int32), (key & 0xFFFFFFFF).astype(np.int32)
+
+
+def build_csr(n, src, dst):
+    """gm_graph CSR + transpose, adjacency sorted (freeze + semi-sort + make_reverse_edges)."""
+    s = np.ascontiguousarray(src, np.int32)
+    d = np.ascontiguousarray(dst, np.int32)
+    m = s.size
+    b = np.empty(n + 1, np.int32); a = np.empty(max(m, 1), np.int32)
+    rb = np.empty(n + 1, np.int32); ra = np.empty(max(m, 1), np.int32)
+    lib().orc_build_csr(n, m, _p(s), _p(d), _p(b), _p(a), _p(rb), _p(ra))
+    return b, a[:m].copy(), rb, ra[:m].copy()
+
+
+def canonical(scc):
+    scc = np.ascontiguousarray(scc, np.int32)
+    out = np.empty_like(scc)
+    lib().orc_canonical(scc.size, _p(scc), _p(out))
+    return out
+
+
+def tarjan_canonical(begin, node_idx):
+    n = begin.size - 1
+    out = np.empty(max(n, 1), np.int32)
+    lib().orc_scc_canonical(n, _p(begin), _p(node_idx), _p(out))
+    return out[:n]
+
+
+def trim1_fixpoint(csr, color, scc):
+    b, a, rb, ra = csr
+    return int(lib().orc_trim1_fixpoint(b.size - 1, _p(b), _p(a), _p(rb), _p(ra), _p(color), _p(scc)))
+
+
+def trim2(csr, color, scc):
+    b, a, rb, ra = csr
+    return int(lib().orc_trim2(b.size - 1, _p(b), _p(a), _p(rb), _p(ra), _p(color), _p(scc)))
+
+
+def wcc_minreach(csr, color):
+    b, a, rb, ra = csr
+    n = b.size - 1
+    out = np.empty(max(n, 1), np.int32)
+    lib().orc_wcc_minreach(n, _p(b), _p(rb), _p(ra), _p(color), _p(out))
+    return out[:n]
+
+
+def choose_pivot(csr, color, c):
+    b, a, rb, ra = csr
+    return int(lib().orc_choose_pivot(b.size - 1, _p(b), _p(rb), _p(color), c))
+
+
+def fw_bw(csr, color, scc, base, pivot, fw_color, bw_color):
+    b, a, rb, ra = csr
+    f = C.c_int64(); w = C.c_int64()
+    s = lib().orc_fw_bw(b.size - 1, _p(b), _p(a), _p(rb), _p(ra), _p(color), _p(scc), base, pivot, fw_color,
+                        bw_color, C.byref(f), C.byref(w))
+    return int(s), f.value, w.value
+
+
+def ref_method2(csr, threads=None, pin=False):
+    """The reference's own method-2 pipeline: (canonical labels, run ms)."""
+    b, a = csr[0], csr[1]
+    n = b.size - 1
+    out = np.empty(max(n, 1), np.int32)
+    ms = C.c_double()
+    th = threads or os.cpu_count() or 1
+    rc = ref().ref_method2(n, a.size, _p(b), _p(a), th, int(pin), _p(out), C.byref(ms))
+    if rc != 0:
+        raise RuntimeError("reference method 2 failed")
+    return canonical(out[:n]), ms.value
+
+
+def ref_tarjan(csr):
+    """The reference's own do_tarjan_all: (canonical labels, run ms)."""
+    b, a = csr[0], csr[1]
+    n = b.size - 1
+    out = np.empty(max(n, 1), np.int32)
+    ms = C.c_double()
+    rc = ref().ref_tarjan(n, a.size, _p(b), _p(a), _p(out), C.byref(ms))
+    if rc != 0:
+        raise RuntimeError("reference Tarjan failed")
+    return canonical(out[:n]), ms.value
