@@ -25,6 +25,7 @@ CU_SOURCES = [
     "scc_state.cu",
     "scc_trim.cu",
     "scc_fb.cu",
+    "scc_reach.cu",
     "scc_wcc.cu",
     "scc_run.cu",
     "scc_gen.cu",

@@ -14,48 +14,29 @@
 // direction, visited bits in a byte per vertex), and a classify pass gives
 // each class the reference's outcome.  A single class (curr_color) is the
 // global step.
-#include "scc_internal.cuh"
+#include "scc_round.cuh"
 
-#define DIR_SHIFT 30
-#define ITEM_MASK 0x3FFFFFFF
-#define WBUF 256          // per-warp push buffer (shared memory)
-#define REACH_THREADS 256
-
-__device__ __forceinline__ uint32_t pivot_hash(uint32_t v) {
-    uint32_t x = v * 0x9E3779B1u;
-    x ^= x >> 16; x *= 0x85EBCA6Bu; x ^= x >> 13;
-    return x;
-}
-
-// Pivot key: (min(in*out, 2^32-2)+1) << 32 | hash(v); never 0, unique per vertex.
-__device__ __forceinline__ unsigned long long pivot_key(const int32_t* __restrict__ begin,
-                                                        const int32_t* __restrict__ r_begin, int32_t v) {
-    unsigned long long outd = (unsigned)(__ldg(begin + v + 1) - __ldg(begin + v));
-    unsigned long long ind = (unsigned)(__ldg(r_begin + v + 1) - __ldg(r_begin + v));
-    unsigned long long prod = outd * ind;
-    if (prod > 0xFFFFFFFEull) prod = 0xFFFFFFFEull;
-    return ((prod + 1ull) << 32) | pivot_hash((uint32_t)v);
-}
-
-struct RoundArgs {
-    const int32_t* begin; const int32_t* node_idx; const int32_t* r_begin; const int32_t* r_node_idx;
-    int32_t* color; int32_t* scc; uint8_t* mark;
-    unsigned long long* slot_key; int32_t* slot_pivot; int32_t* slot_fw; int32_t* slot_bw;
-    int64_t colour_cap;
-    int32_t* ctr;
-    const int32_t* live; int32_t live_count;
-    int32_t only_color;   // INT32_MIN = every class
-    int32_t use_only;
-};
-
-__global__ void k_slot_reset(RoundArgs a) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.live_count; i += (int64_t)gridDim.x * blockDim.x) {
+// Reset the per-colour pivot slots of the classes present and total the
+// in+out degree of the vertices this round will traverse (the direction rule
+// of the traversal compares frontier edges against it).
+__global__ void k_slot_reset(RoundArgs a, int reset_slots) {
+    unsigned long long deg = 0;
+    int64_t limit = (((int64_t)a.live_count + 31) / 32) * 32;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i >= a.live_count) continue;
         int32_t v = a.live[i];
         int32_t c = a.color[v];
-        if (c == SCC_COLOR_DONE) continue;
-        a.slot_key[c + 1] = 0ull;
-        a.slot_pivot[c + 1] = SCC_NIL_NODE;
+        if (c == SCC_COLOR_DONE || (a.use_only && c != a.only_color)) continue;
+        deg += (unsigned)(__ldg(a.begin + v + 1) - __ldg(a.begin + v)) +
+               (unsigned)(__ldg(a.r_begin + v + 1) - __ldg(a.r_begin + v));
+        if (reset_slots) {
+            a.slot_key[c + 1] = 0ull;
+            a.slot_pivot[c + 1] = SCC_NIL_NODE;
+        }
     }
+    for (int o = 16; o > 0; o >>= 1) deg += __shfl_down_sync(0xFFFFFFFFu, deg, o);
+    if ((threadIdx.x & 31) == 0 && deg)
+        atomicAdd(reinterpret_cast<unsigned long long*>(a.ctr + CTR_LIVE_EDGES), deg);
 }
 
 __global__ void k_pivot_key(RoundArgs a) {
@@ -93,95 +74,6 @@ __global__ void k_pivot_pick(RoundArgs a, int32_t* q) {
 
 __global__ void k_pivot_forced(RoundArgs a, int32_t v, int32_t* q) {
     if (blockIdx.x == 0 && threadIdx.x == 0) seed_pivot(a, v, a.color[v], q);
-}
-
-// ------------------------------------------------------------------ one BFS level
-struct WarpPush {
-    int32_t* buf;     // this warp's shared buffer
-    int32_t count;    // warp-uniform
-};
-
-__device__ __forceinline__ void warp_flush(WarpPush& wp, int32_t* __restrict__ qout, int32_t* __restrict__ qlen) {
-    int lane = threadIdx.x & 31;
-    __syncwarp();
-    if (wp.count > 0) {
-        int32_t base = 0;
-        if (lane == 0) base = atomicAdd(qlen, wp.count);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        for (int j = lane; j < wp.count; j += 32) qout[base + j] = wp.buf[j];
-    }
-    __syncwarp();
-    wp.count = 0;
-}
-
-__device__ __forceinline__ void warp_push(WarpPush& wp, bool p, int32_t item, int32_t* __restrict__ qout,
-                                          int32_t* __restrict__ qlen) {
-    int lane = threadIdx.x & 31;
-    unsigned bal = __ballot_sync(0xFFFFFFFFu, p);
-    if (p) wp.buf[wp.count + __popc(bal & ((1u << lane) - 1u))] = item;
-    wp.count += __popc(bal);
-    if (wp.count > WBUF - 32) warp_flush(wp, qout, qlen);
-}
-
-// Claim w for direction `dir` inside colour c; true if this thread claimed it.
-__device__ __forceinline__ bool visit(const RoundArgs& a, int32_t w, int32_t c, int dir) {
-    unsigned bit = 1u << dir;
-    if (a.mark[w] & bit) return false;
-    if (__ldg(a.color + w) != c) return false;
-    unsigned sh = (unsigned)(w & 3) * 8u;
-    unsigned old = atomicOr(reinterpret_cast<unsigned*>(a.mark + (w & ~3)), bit << sh);
-    return ((old >> sh) & bit) == 0u;
-}
-
-__global__ void __launch_bounds__(REACH_THREADS) k_reach_level(RoundArgs a, const int32_t* __restrict__ qin,
-                                                                int32_t nin, int32_t* __restrict__ qout) {
-    __shared__ int32_t sbuf[REACH_THREADS / 32][WBUF];
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    WarpPush wp{sbuf[wid], 0};
-    int32_t* qlen = a.ctr + CTR_QLEN;
-    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    int64_t groups = ((int64_t)nin + 31) >> 5;
-    for (int64_t gi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; gi < groups; gi += nwarps) {
-        int64_t idx = gi * 32 + lane;
-        int32_t v = 0, dir = 0, b = 0, e = 0, c = 0;
-        if (idx < nin) {
-            int32_t it = qin[idx];
-            v = it & ITEM_MASK;
-            dir = (it >> DIR_SHIFT) & 1;
-            const int32_t* off = dir ? a.r_begin : a.begin;
-            b = __ldg(off + v);
-            e = __ldg(off + v + 1);
-            c = __ldg(a.color + v);
-        }
-        int32_t deg = e - b;
-        // high-degree vertices: the whole warp strides the adjacency
-        unsigned big = __ballot_sync(0xFFFFFFFFu, deg > 32);
-        while (big) {
-            int l = __ffs(big) - 1;
-            big &= big - 1;
-            int32_t bb = __shfl_sync(0xFFFFFFFFu, b, l), be = __shfl_sync(0xFFFFFFFFu, e, l);
-            int32_t bc = __shfl_sync(0xFFFFFFFFu, c, l), bd = __shfl_sync(0xFFFFFFFFu, dir, l);
-            const int32_t* adj = bd ? a.r_node_idx : a.node_idx;
-            for (int32_t k0 = bb; k0 < be; k0 += 32) {
-                int32_t k = k0 + lane;
-                bool p = false;
-                int32_t w = 0;
-                if (k < be) { w = __ldg(adj + k); p = visit(a, w, bc, bd); }
-                warp_push(wp, p, w | (bd << DIR_SHIFT), qout, qlen);
-            }
-        }
-        // low-degree vertices: each lane walks its own list, warp-uniform trip count
-        int32_t mydeg = deg <= 32 ? deg : 0;
-        int32_t maxd = __reduce_max_sync(0xFFFFFFFFu, (unsigned)mydeg);
-        const int32_t* adj = dir ? a.r_node_idx : a.node_idx;
-        for (int32_t j = 0; j < maxd; ++j) {
-            bool p = false;
-            int32_t w = 0;
-            if (j < mydeg) { w = __ldg(adj + b + j); p = visit(a, w, c, dir); }
-            warp_push(wp, p, w | (dir << DIR_SHIFT), qout, qlen);
-        }
-    }
-    warp_flush(wp, qout, qlen);
 }
 
 // ------------------------------------------------------------------ classify
@@ -224,24 +116,8 @@ static RoundArgs round_args(const scc_graph* g, scc_state* s) {
     a.ctr = s->ctr;
     a.live = s->live; a.live_count = s->live_count;
     a.only_color = 0; a.use_only = 0;
+    a.pivot_score = nullptr;
     return a;
-}
-
-// Run reachability from the queue in s->qa (length qlen) to completion.
-static int reach_to_completion(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen) {
-    int32_t* qin = s->qa;
-    int32_t* qout = s->qb;
-    while (qlen > 0) {
-        SCC_TRY(scc_zero_counters(s, CTR_QLEN, 1));
-        unsigned blocks = scc_blocks((int64_t)qlen, REACH_THREADS, 148 * 8);
-        k_reach_level<<<blocks, REACH_THREADS, 0, s->stream>>>(a, qin, qlen, qout);
-        SCC_LAUNCHED(s);
-        s->traversal_steps++;
-        SCC_TRY(scc_sync_counters(s));
-        qlen = s->h_ctr[CTR_QLEN];
-        int32_t* t = qin; qin = qout; qout = t;
-    }
-    return SCC_OK;
 }
 
 // One FW-BW round over every live class (only_color == INT32_MIN) or one class.
@@ -259,12 +135,13 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
     unsigned blocks = scc_blocks(s->live_count);
     SCC_TRY(scc_zero_counters(s, CTR_COUNT, 4));
     SCC_TRY(scc_zero_counters(s, CTR_NUM_CLASSES, 1));
+    SCC_TRY(scc_zero_counters(s, CTR_LIVE_EDGES, 2));
+    k_slot_reset<<<blocks, SCC_THREADS, 0, s->stream>>>(a, forced_pivot < 0 ? 1 : 0);
+    SCC_LAUNCHED(s);
     if (forced_pivot >= 0) {
         k_pivot_forced<<<1, 32, 0, s->stream>>>(a, forced_pivot, s->qa);
         SCC_LAUNCHED(s);
     } else {
-        k_slot_reset<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
-        SCC_LAUNCHED(s);
         k_pivot_key<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
         SCC_LAUNCHED(s);
         k_pivot_pick<<<blocks, SCC_THREADS, 0, s->stream>>>(a, s->qa);
@@ -274,7 +151,7 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
     if (s->h_ctr[CTR_ERROR]) SCC_TRY(scc_check_device_error(s));
     int32_t qlen = s->h_ctr[CTR_QLEN];
     if (active) *active = s->h_ctr[CTR_NUM_CLASSES];
-    SCC_TRY(reach_to_completion(g, s, a, qlen));
+    SCC_TRY(scc_impl_reach(g, s, a, qlen));
     SCC_TRY(scc_zero_counters(s, CTR_COUNT, 3));
     k_classify<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
     SCC_LAUNCHED(s);
@@ -285,6 +162,10 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
 
 // Resolve every live class to SCCs: trim, FW-BW round, repeat (the device
 // replacement for start_workers_fw_bw[_dfs], src/scc_fb_seq2.cc:292-351).
+// Each round: peel (trim1 inside colours), split every class into its weak
+// components (so independent pieces get their own pivot), then one FW-BW
+// round over all classes at once.  Every class loses at least its pivot's SCC
+// per round, so the loop ends.
 int scc_impl_resolve_all(const scc_graph* g, scc_state* s) {
     if (s->live_count < 0) SCC_TRY(scc_impl_compact_live(g, s, true));
     for (int round = 0; round < (1 << 30); ++round) {
@@ -292,9 +173,16 @@ int scc_impl_resolve_all(const scc_graph* g, scc_state* s) {
         SCC_TRY(scc_impl_trim1(g, s, true, &t));
         SCC_TRY(scc_impl_compact_live(g, s, false));
         if (s->live_count == 0) break;
+        int32_t classes = 0;
+        SCC_TRY(scc_impl_uf_split(g, s, &classes));
+        int32_t live_before = s->live_count;
         int32_t found = 0, act = 0;
         SCC_TRY(scc_impl_fb_round(g, s, INT32_MIN, -1, &found, &act));
         SCC_TRY(scc_impl_compact_live(g, s, false));
+        if (scc_trace_on())
+            fprintf(stderr, "[scc] round %d: trimmed=%d live=%d classes=%d scc_found=%d left=%d\n", round, t,
+                    live_before, classes, found, s->live_count);
+        s->fb_rounds++;
         if (s->live_count == 0) break;
         if (found == 0) { scc_set_error("FW-BW round made no progress"); return SCC_ERR_STATE; }
     }

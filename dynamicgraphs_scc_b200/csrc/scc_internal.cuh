@@ -59,7 +59,13 @@ enum {
     CTR_SPARE2,
     CTR_SPARE3,
     CTR_SPARE4,
-    CTR_MAX = 32
+    CTR_EDGES = 16,      // u64 (slots 16-17): edges of the next top-down frontier
+    CTR_LIVE_EDGES = 18, // u64 (slots 18-19): in+out degree of the vertices being traversed
+    // asynchronous traversal queue counters, one 128-byte line each (polled by idle warps)
+    CTR_AHEAD = 32,
+    CTR_ATAIL = 64,
+    CTR_AWORK = 96,
+    CTR_MAX = 128
 };
 
 // device error codes written to CTR_ERROR
@@ -73,6 +79,7 @@ struct scc_state {
     cudaStream_t stream = nullptr;
     int kernels = 0;                 // kernels launched (statistics)
     int64_t traversal_steps = 0;
+    int32_t fb_rounds = 0;           // recursion rounds (statistics)
 
     int32_t* color = nullptr;        // G_Color [n]
     int32_t* scc = nullptr;          // G_SCC   [n]
@@ -82,6 +89,10 @@ struct scc_state {
     int32_t* live_tmp = nullptr;     // [n] scratch list
     int32_t* qa = nullptr;           // [2n+64] traversal queue A
     int32_t* qb = nullptr;           // [2n+64] traversal queue B
+    int32_t* aq = nullptr;           // [2n+64] asynchronous traversal queue, kept at -1 between uses
+    int32_t* uf = nullptr;           // [n] union-find parents (weak-component split)
+    int32_t* hq = nullptr;           // [2n+64] high-degree items deferred by a top-down level
+    long long* hoff = nullptr;       // [2n+64] prefix of their degrees
     uint8_t* mark = nullptr;         // [n rounded to 4] reachability marks (bit0 FW, bit1 BW)
     int32_t* aux = nullptr;          // [n] per-vertex scratch (trim2 mates, pivot slots...)
     int32_t* block_sums = nullptr;   // scan scratch
@@ -126,6 +137,8 @@ int scc_impl_ensure_colour_cap(scc_state* s, int64_t need);
 int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int32_t forced_pivot,
                       int32_t* scc_found, int32_t* active_classes);
 int scc_impl_wcc(const scc_graph* g, scc_state* s);
+int scc_impl_uf_split(const scc_graph* g, scc_state* s, int32_t* num_classes);
+bool scc_trace_on();
 int scc_impl_resolve_all(const scc_graph* g, scc_state* s);
 int scc_impl_get_live_host(scc_state* s, std::vector<int32_t>& out);
 int scc_impl_count_colour(scc_state* s, int32_t color, int32_t* count);

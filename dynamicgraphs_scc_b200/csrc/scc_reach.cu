@@ -1,0 +1,492 @@
+// Forward/backward reachability inside colour classes, the traversal under
+// every FW-BW step (fw_trim_global / bw_trim_global, src/scc_fb_global.cc:32-130,
+// and the per-item searches of src/scc_fb_seq2.cc:10-177).
+//
+// Items are (vertex | direction << 30); direction 0 walks out-edges (FW),
+// 1 walks in-edges (BW).  A vertex is claimed once per direction with an
+// atomicOr on its mark byte, so FW and BW of every class advance together.
+// Three execution modes, chosen per step by the host from the frontier size:
+//
+//  * top-down level (k_reach_level): one launch per BFS level; a warp takes 32
+//    items, vertices with more than 32 neighbours are expanded by the whole
+//    warp (coalesced adjacency reads), the rest lane by lane; new items go to
+//    a per-warp shared-memory buffer and reach the global queue in batches;
+//  * bottom-up sweep (k_reach_bottomup): when the frontier is a large share of
+//    the live vertices (the "RD" state of gm_bfs_template.h:418-487), every
+//    unvisited live vertex looks for an already visited parent among its
+//    in-neighbours (FW) / out-neighbours (BW) and stops at the first one;
+//  * asynchronous drain (k_reach_async): once the frontier has stayed narrow
+//    for a few levels (long-diameter inputs such as grids and long cycles),
+//    one persistent launch finishes the traversal with no level barriers and
+//    no host round trips.  Each warp works LIFO from its own shared-memory
+//    list and spills surplus items to a global queue that idle warps drain.
+//    A global `work` counter (items claimed but not yet expanded) detects the
+//    end.  Every wait is bounded: past its limit a warp records
+//    SCC_DEVERR_WAIT_LIMIT and returns, and the host reports SCC_ERR_TIMEOUT.
+#include <stdlib.h>
+#include "scc_round.cuh"
+
+#define BU_DIV 24               // bottom-up when frontier > 2*live/BU_DIV
+#define ASYNC_MAX (1 << 16)     // narrow frontier
+#define ASYNC_AFTER 2           // consecutive narrow levels before draining asynchronously
+#define ASYNC_EMPTY (-1)
+#define ASYNC_IDLE_LIMIT (1 << 22)
+#define ASYNC_SLOT_LIMIT (1 << 20)
+#define ASYNC_SPILL_KEEP 64
+
+// ------------------------------------------------------------------ warp expansion
+// Expand one item per lane (valid lanes only); push(p, item) is warp-collective.
+// Items whose degree exceeds HUGE_DEG are handed to k_reach_huge (edge-parallel
+// over the whole grid) when huge_list is given, so one hub never serialises a level.
+#define HUGE_DEG 4096
+template <class Push>
+__device__ __forceinline__ void expand_warp(const RoundArgs& a, bool valid, int32_t it, Push& push,
+                                            int32_t* huge_list = nullptr, int32_t* huge_cnt = nullptr) {
+    int lane = threadIdx.x & 31;
+    int32_t v = 0, dir = 0, b = 0, e = 0, c = 0;
+    if (valid) {
+        v = it & ITEM_MASK;
+        dir = (it >> DIR_SHIFT) & 1;
+        const int32_t* off = dir ? a.r_begin : a.begin;
+        b = __ldg(off + v);
+        e = __ldg(off + v + 1);
+        c = __ldg(a.color + v);
+        if (huge_list && e - b > HUGE_DEG) {
+            huge_list[atomicAdd(huge_cnt, 1)] = it;
+            e = b;
+        }
+    }
+    int32_t deg = e - b;
+    unsigned big = __ballot_sync(0xFFFFFFFFu, deg > 32);
+    while (big) {
+        int l = __ffs(big) - 1;
+        big &= big - 1;
+        int32_t bb = __shfl_sync(0xFFFFFFFFu, b, l), be = __shfl_sync(0xFFFFFFFFu, e, l);
+        int32_t bc = __shfl_sync(0xFFFFFFFFu, c, l), bd = __shfl_sync(0xFFFFFFFFu, dir, l);
+        const int32_t* adj = bd ? a.r_node_idx : a.node_idx;
+        for (int32_t k0 = bb; k0 < be; k0 += 32) {
+            int32_t k = k0 + lane;
+            bool p = false;
+            int32_t w = 0;
+            if (k < be) { w = __ldg(adj + k); p = visit(a, w, bc, bd); }
+            push(p, w | (bd << DIR_SHIFT));
+        }
+    }
+    // Low-degree lists, four neighbours at a time: the adjacency loads, then the
+    // mark and colour loads, then the claims are each issued together, so a hop
+    // costs three memory round trips rather than three per neighbour.
+    int32_t mydeg = deg <= 32 ? deg : 0;
+    int32_t maxd = (int32_t)__reduce_max_sync(0xFFFFFFFFu, (unsigned)mydeg);
+    const int32_t* adj = dir ? a.r_node_idx : a.node_idx;
+    const unsigned bit = 1u << dir;
+    for (int32_t j0 = 0; j0 < maxd; j0 += 4) {
+        int32_t w[4];
+        bool p[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            p[u] = (j0 + u) < mydeg;
+            w[u] = p[u] ? __ldg(adj + b + j0 + u) : 0;
+        }
+        unsigned mk[4];
+        int32_t col[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            mk[u] = p[u] ? (unsigned)*(volatile uint8_t*)(a.mark + w[u]) : bit;
+            col[u] = p[u] ? __ldg(a.color + w[u]) : c;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            p[u] = p[u] && !(mk[u] & bit) && col[u] == c;
+            if (p[u]) {
+                unsigned sh = (unsigned)(w[u] & 3) * 8u;
+                unsigned old = atomicOr(reinterpret_cast<unsigned*>(a.mark + (w[u] & ~3)), bit << sh);
+                p[u] = ((old >> sh) & bit) == 0u;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) push(p[u], w[u] | (dir << DIR_SHIFT));
+    }
+}
+
+// ------------------------------------------------------------------ level mode
+struct GlobalPush {
+    int32_t* buf;          // warp's shared buffer
+    int32_t count;         // warp-uniform
+    int32_t* qout;
+    int32_t* qlen;
+    const int32_t* off_fw; // degree of pushed items (frontier edge count), nullptr = skip
+    const int32_t* off_bw;
+    unsigned long long edges;   // per lane
+    __device__ __forceinline__ void finish(unsigned long long* total) {
+        flush();
+        if (off_fw) {
+            unsigned long long e = edges;
+            for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xFFFFFFFFu, e, o);
+            if ((threadIdx.x & 31) == 0 && e) atomicAdd(total, e);
+        }
+    }
+    __device__ __forceinline__ void flush() {
+        int lane = threadIdx.x & 31;
+        __syncwarp();
+        if (count > 0) {
+            int32_t base = 0;
+            if (lane == 0) base = atomicAdd(qlen, count);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            for (int j = lane; j < count; j += 32) qout[base + j] = buf[j];
+        }
+        __syncwarp();
+        count = 0;
+    }
+    __device__ __forceinline__ void operator()(bool p, int32_t item) {
+        int lane = threadIdx.x & 31;
+        unsigned bal = __ballot_sync(0xFFFFFFFFu, p);
+        if (p) {
+            buf[count + __popc(bal & ((1u << lane) - 1u))] = item;
+            if (off_fw) {
+                int32_t w = item & ITEM_MASK;
+                const int32_t* off = (item >> DIR_SHIFT) ? off_bw : off_fw;
+                edges += (unsigned)(__ldg(off + w + 1) - __ldg(off + w));
+            }
+        }
+        count += __popc(bal);
+        if (count > WBUF - 32) flush();
+    }
+};
+
+__global__ void __launch_bounds__(REACH_THREADS) k_reach_level(RoundArgs a, const int32_t* __restrict__ qin,
+                                                                int32_t nin, int32_t* __restrict__ qout,
+                                                                int32_t* __restrict__ huge_list) {
+    __shared__ int32_t sbuf[REACH_THREADS / 32][WBUF];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    GlobalPush push{sbuf[wid], 0, qout, a.ctr + CTR_QLEN, a.begin, a.r_begin, 0ull};
+    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    int64_t groups = ((int64_t)nin + 31) >> 5;
+    for (int64_t gi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; gi < groups; gi += nwarps) {
+        int64_t idx = gi * 32 + lane;
+        bool valid = idx < nin;
+        int32_t it = valid ? qin[idx] : 0;
+        expand_warp(a, valid, it, push, huge_list, a.ctr + CTR_SPARE4);
+    }
+    push.finish(reinterpret_cast<unsigned long long*>(a.ctr + CTR_EDGES));
+}
+
+// Inclusive prefix of the deferred items' degrees (one block; hoff[j] = end of item j).
+__global__ void k_huge_prefix(RoundArgs a, const int32_t* __restrict__ list, int32_t cnt,
+                              long long* __restrict__ hoff) {
+    __shared__ long long part[1024];
+    int t = threadIdx.x;
+    int32_t per = (cnt + 1023) / 1024;
+    int32_t b = t * per, e = min(cnt, b + per);
+    long long s = 0;
+    for (int32_t j = b; j < e; ++j) {
+        int32_t it = list[j], v = it & ITEM_MASK;
+        const int32_t* off = (it >> DIR_SHIFT) ? a.r_begin : a.begin;
+        s += __ldg(off + v + 1) - __ldg(off + v);
+    }
+    part[t] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        long long x = (t >= o) ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += x;
+        __syncthreads();
+    }
+    long long run = (t == 0) ? 0 : part[t - 1];
+    for (int32_t j = b; j < e; ++j) {
+        int32_t it = list[j], v = it & ITEM_MASK;
+        const int32_t* off = (it >> DIR_SHIFT) ? a.r_begin : a.begin;
+        run += __ldg(off + v + 1) - __ldg(off + v);
+        hoff[j] = run;
+    }
+}
+
+// Edge-parallel expansion of the deferred high-degree items: thread t takes
+// edge t of the concatenated adjacency lists (consecutive lanes, consecutive edges).
+__global__ void __launch_bounds__(REACH_THREADS) k_reach_huge(RoundArgs a, const int32_t* __restrict__ list,
+                                                               int32_t cnt, const long long* __restrict__ hoff,
+                                                               int32_t* __restrict__ qout) {
+    __shared__ int32_t sbuf[REACH_THREADS / 32][WBUF];
+    int wid = threadIdx.x >> 5;
+    GlobalPush push{sbuf[wid], 0, qout, a.ctr + CTR_QLEN, a.begin, a.r_begin, 0ull};
+    long long total = hoff[cnt - 1];
+    long long stride = (long long)gridDim.x * blockDim.x;
+    long long limit = ((total + 31) / 32) * 32;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < limit; t += stride) {
+        bool p = false;
+        int32_t w = 0, d = 0;
+        if (t < total) {
+            int32_t lo = 0, hi = cnt - 1;
+            while (lo < hi) { int32_t mid = (lo + hi) >> 1; if (hoff[mid] > t) hi = mid; else lo = mid + 1; }
+            int32_t it = list[lo], v = it & ITEM_MASK;
+            d = (it >> DIR_SHIFT) & 1;
+            long long start = lo ? hoff[lo - 1] : 0;
+            const int32_t* off = d ? a.r_begin : a.begin;
+            const int32_t* adj = d ? a.r_node_idx : a.node_idx;
+            w = __ldg(adj + __ldg(off + v) + (t - start));
+            p = visit(a, w, __ldg(a.color + v), d);
+        }
+        push(p, w | (d << DIR_SHIFT));
+    }
+    push.finish(reinterpret_cast<unsigned long long*>(a.ctr + CTR_EDGES));
+}
+
+// ------------------------------------------------------------------ bottom-up mode
+__device__ __forceinline__ bool has_marked_parent(const RoundArgs& a, const int32_t* __restrict__ off,
+                                                  const int32_t* __restrict__ adj, int32_t v, int32_t c,
+                                                  unsigned bit) {
+    int32_t b = __ldg(off + v), e = __ldg(off + v + 1);
+    for (int32_t k = b; k < e; ++k) {
+        int32_t u = __ldg(adj + k);
+        if ((*(volatile uint8_t*)(a.mark + u) & bit) && __ldg(a.color + u) == c) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(REACH_THREADS) k_reach_bottomup(RoundArgs a, int32_t* __restrict__ qout) {
+    __shared__ int32_t sbuf[REACH_THREADS / 32][WBUF];
+    int wid = threadIdx.x >> 5;
+    GlobalPush push{sbuf[wid], 0, qout, a.ctr + CTR_QLEN, nullptr, nullptr, 0ull};
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t limit = (((int64_t)a.live_count + 31) / 32) * 32;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += stride) {
+        bool p0 = false, p1 = false;
+        int32_t v = 0;
+        if (i < a.live_count) {
+            v = a.live[i];
+            int32_t c = __ldg(a.color + v);
+            if (c != SCC_COLOR_DONE && (!a.use_only || c == a.only_color)) {
+                unsigned m = *(volatile uint8_t*)(a.mark + v);
+                if (!(m & 1u)) p0 = has_marked_parent(a, a.r_begin, a.r_node_idx, v, c, 1u);
+                if (!(m & 2u)) p1 = has_marked_parent(a, a.begin, a.node_idx, v, c, 2u);
+                if (p0 || p1) {
+                    unsigned sh = (unsigned)(v & 3) * 8u;
+                    unsigned bits = (p0 ? 1u : 0u) | (p1 ? 2u : 0u);
+                    unsigned old = atomicOr(reinterpret_cast<unsigned*>(a.mark + (v & ~3)), bits << sh);
+                    // push only directions this thread newly set
+                    p0 = p0 && !((old >> sh) & 1u);
+                    p1 = p1 && !((old >> sh) & 2u);
+                }
+            }
+        }
+        push(p0, v);
+        push(p1, v | (1 << DIR_SHIFT));
+    }
+    push.flush();
+}
+
+// ------------------------------------------------------------------ asynchronous mode
+struct LocalPush {
+    int32_t* buf;          // warp's shared list
+    int32_t count;         // warp-uniform
+    int32_t pushed;        // items added since the last work-counter update
+    int32_t* q; int32_t* tail; int32_t* work; int64_t qcap; int32_t* err;
+    __device__ __forceinline__ void spill(int32_t keep) {
+        int lane = threadIdx.x & 31;
+        __syncwarp();
+        int32_t ns = count - keep;
+        if (ns > 0) {
+            int32_t base = 0;
+            if (lane == 0) {
+                if (pushed) { atomicAdd(work, pushed); }
+                base = atomicAdd(tail, ns);
+                if ((int64_t)base + ns > qcap) atomicExch(err, SCC_DEVERR_QUEUE_OVERFLOW);
+            }
+            pushed = 0;
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if ((int64_t)base + ns <= qcap)
+                for (int j = lane; j < ns; j += 32) *(volatile int32_t*)(q + base + j) = buf[keep + j];
+            count = keep;
+        }
+        __syncwarp();
+    }
+    __device__ __forceinline__ void operator()(bool p, int32_t item) {
+        int lane = threadIdx.x & 31;
+        unsigned bal = __ballot_sync(0xFFFFFFFFu, p);
+        if (p) buf[count + __popc(bal & ((1u << lane) - 1u))] = item;
+        int32_t k = __popc(bal);
+        count += k;
+        pushed += k;
+        if (count > WBUF - 32) spill(ASYNC_SPILL_KEEP);
+    }
+};
+
+__device__ __forceinline__ int32_t ld_volatile(const int32_t* p) { return *(const volatile int32_t*)p; }
+
+__global__ void __launch_bounds__(REACH_THREADS) k_reach_async(RoundArgs a, int32_t* __restrict__ q, int64_t qcap) {
+    __shared__ int32_t sbuf[REACH_THREADS / 32][WBUF];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int32_t* head = a.ctr + CTR_AHEAD;
+    int32_t* tail = a.ctr + CTR_ATAIL;
+    int32_t* work = a.ctr + CTR_AWORK;
+    int32_t* err = a.ctr + CTR_ERROR;
+    LocalPush push{sbuf[wid], 0, 0, q, tail, work, qcap, err};
+    int idle = 0;
+    int32_t last_work = -1;
+    while (true) {
+        if (push.count == 0) {
+            int32_t got = 0, base = 0;
+            if (lane == 0) {
+                int32_t t = ld_volatile(tail), h = ld_volatile(head);
+                if (h < t) {
+                    int32_t k = min(32, t - h);
+                    if (atomicCAS(head, h, h + k) == h) { got = k; base = h; }
+                }
+            }
+            got = __shfl_sync(0xFFFFFFFFu, got, 0);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (got == 0) {
+                ++idle;
+                if ((idle & 7) == 1) {
+                    int32_t w = 1, e = 0;
+                    if (lane == 0) { w = ld_volatile(work); e = ld_volatile(err); }
+                    w = __shfl_sync(0xFFFFFFFFu, w, 0);
+                    e = __shfl_sync(0xFFFFFFFFu, e, 0);
+                    if (w == 0 || e != 0) break;
+                    // the limit bounds a stall, not a long traversal: progress elsewhere resets it
+                    if (w != last_work) { last_work = w; idle = 1; }
+                }
+                if (idle > ASYNC_IDLE_LIMIT) {
+                    if (lane == 0) { atomicExch(err, SCC_DEVERR_WAIT_LIMIT); atomicExch(a.ctr + CTR_ERROR_INFO, 1); }
+                    break;
+                }
+                __nanosleep(idle < 16 ? 100 : 500);
+                continue;
+            }
+            idle = 0;
+            int32_t item = ASYNC_EMPTY;
+            if (lane < got) {
+                volatile int32_t* slot = q + base + lane;
+                int spins = 0;
+                while ((item = *slot) == ASYNC_EMPTY && spins < ASYNC_SLOT_LIMIT) { spins++; __nanosleep(20); }
+                if (item != ASYNC_EMPTY) *slot = ASYNC_EMPTY;
+            }
+            if (__any_sync(0xFFFFFFFFu, lane < got && item == ASYNC_EMPTY)) {
+                if (lane == 0) { atomicExch(err, SCC_DEVERR_WAIT_LIMIT); atomicExch(a.ctr + CTR_ERROR_INFO, 2); }
+                break;
+            }
+            if (lane < got) push.buf[lane] = item;
+            __syncwarp();
+            push.count = got;
+        }
+        int32_t k = min(32, push.count);
+        int32_t it = (lane < k) ? push.buf[push.count - k + lane] : 0;
+        __syncwarp();
+        push.count -= k;
+        expand_warp(a, lane < k, it, push);
+        int32_t delta = push.pushed - k;
+        if (lane == 0 && delta != 0) atomicAdd(work, delta);
+        push.pushed = 0;
+        // keep one iteration's worth (this warp's own continuation), share the rest
+        if (push.count > 32) push.spill(32);
+    }
+}
+
+// ------------------------------------------------------------------ host driver
+bool scc_trace_on() {
+    static int t = -1;
+    if (t < 0) { const char* e = getenv("SCC_TRACE"); t = (e && *e && *e != '0') ? 1 : 0; }
+    return t == 1;
+}
+
+static int async_blocks(int device) {
+    static int cached[64] = {0};
+    if (device >= 0 && device < 64 && cached[device]) return cached[device];
+    int sms = 148, per = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_reach_async, REACH_THREADS, 0);
+    if (per < 1) per = 1;
+    // every block must be resident (warps wait on each other's items); two per SM
+    // (16 warps) cover a narrow frontier without flooding the queue with pollers
+    if (per > 2) per = 2;
+    int b = sms * per;
+    if (device >= 0 && device < 64) cached[device] = b;
+    return b;
+}
+
+static double now_ms() {
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return t.tv_sec * 1e3 + t.tv_nsec * 1e-6;
+}
+
+// Direction choice (Beamer's rule as in the reference's BFS state machine,
+// gm_bfs_template.h:418-487): go bottom-up when the next frontier's edges
+// times BU_ALPHA exceed the edges of the vertices being traversed; stay
+// bottom-up while the frontier holds more than 2*live/BU_DIV items.
+#define BU_ALPHA 14
+
+int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen) {
+    int32_t* qin = s->qa;
+    int32_t* qout = s->qb;
+    int64_t live2 = 2LL * (a.live_count > 0 ? a.live_count : 1);
+    unsigned long long live_edges = *reinterpret_cast<unsigned long long*>(s->h_ctr + CTR_LIVE_EDGES);
+    if (live_edges == 0) live_edges = 1;
+    int narrow = 0;
+    bool bottom_up = false;
+    double t0 = scc_trace_on() ? now_ms() : 0.0;
+    while (qlen > 0) {
+        const char* mode;
+        if (bottom_up) {
+            SCC_TRY(scc_zero_counters(s, CTR_QLEN, 1));
+            k_reach_bottomup<<<scc_blocks(a.live_count, REACH_THREADS, 148 * 16), REACH_THREADS, 0, s->stream>>>(a, qout);
+            SCC_LAUNCHED(s);
+            narrow = 0;
+            mode = "bottom-up";
+        } else if (qlen <= ASYNC_MAX && narrow >= ASYNC_AFTER) {
+            int64_t qcap = 2LL * s->n + 64;
+            SCC_CUDA(cudaMemcpyAsync(s->aq, qin, sizeof(int32_t) * (size_t)qlen, cudaMemcpyDeviceToDevice, s->stream));
+            int32_t init[CTR_AWORK - CTR_AHEAD + 1] = {0};   // head, tail, work on separate lines
+            init[CTR_ATAIL - CTR_AHEAD] = qlen;
+            init[CTR_AWORK - CTR_AHEAD] = qlen;
+            SCC_CUDA(cudaMemcpyAsync(s->ctr + CTR_AHEAD, init, sizeof(init), cudaMemcpyHostToDevice, s->stream));
+            k_reach_async<<<async_blocks(s->device), REACH_THREADS, 0, s->stream>>>(a, s->aq, qcap);
+            SCC_LAUNCHED(s);
+            s->traversal_steps++;
+            SCC_TRY(scc_sync_counters(s));
+            if (scc_trace_on()) {
+                double t1 = now_ms();
+                fprintf(stderr, "[scc] reach async seeds=%d spilled=%d %.3f ms\n", qlen, s->h_ctr[CTR_ATAIL], t1 - t0);
+            }
+            if (s->h_ctr[CTR_ERROR]) {
+                // leave the queue clean for the next traversal, then report
+                SCC_CUDA(cudaMemsetAsync(s->aq, 0xFF, sizeof(int32_t) * (size_t)qcap, s->stream));
+                return scc_check_device_error(s);
+            }
+            return SCC_OK;
+        } else {
+            SCC_TRY(scc_zero_counters(s, CTR_QLEN, 1));
+            SCC_TRY(scc_zero_counters(s, CTR_SPARE4, 1));
+            SCC_TRY(scc_zero_counters(s, CTR_EDGES, 2));
+            k_reach_level<<<scc_blocks((int64_t)qlen, REACH_THREADS, 148 * 8), REACH_THREADS, 0, s->stream>>>(
+                a, qin, qlen, qout, s->hq);
+            SCC_LAUNCHED(s);
+            SCC_TRY(scc_sync_counters(s));
+            int32_t nhuge = s->h_ctr[CTR_SPARE4];
+            if (nhuge > 0) {
+                k_huge_prefix<<<1, 1024, 0, s->stream>>>(a, s->hq, nhuge, s->hoff);
+                SCC_LAUNCHED(s);
+                k_reach_huge<<<148 * 8, REACH_THREADS, 0, s->stream>>>(a, s->hq, nhuge, s->hoff, qout);
+                SCC_LAUNCHED(s);
+            }
+            mode = nhuge > 0 ? "top-down+huge" : "top-down";
+        }
+        s->traversal_steps++;
+        SCC_TRY(scc_sync_counters(s));
+        int32_t next = s->h_ctr[CTR_QLEN];
+        if (bottom_up) {
+            bottom_up = (int64_t)next * BU_DIV > live2;
+        } else {
+            unsigned long long fe = *reinterpret_cast<unsigned long long*>(s->h_ctr + CTR_EDGES);
+            bottom_up = fe * BU_ALPHA > live_edges;
+        }
+        if (scc_trace_on()) {
+            double t1 = now_ms();
+            fprintf(stderr, "[scc] reach %s in=%d out=%d %.3f ms\n", mode, qlen, next, t1 - t0);
+            t0 = t1;
+        }
+        narrow = (!bottom_up && next <= ASYNC_MAX) ? narrow + 1 : 0;
+        qlen = next;
+        int32_t* t = qin; qin = qout; qout = t;
+    }
+    return SCC_OK;
+}

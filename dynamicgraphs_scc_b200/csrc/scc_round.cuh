@@ -1,0 +1,48 @@
+// Shared definitions for one FW-BW round: arguments, pivot key, visit/claim.
+#pragma once
+#include "scc_internal.cuh"
+
+#define DIR_SHIFT 30
+#define ITEM_MASK 0x3FFFFFFF
+#define REACH_THREADS 256
+#define WBUF 256          // per-warp shared-memory buffer (items)
+
+struct RoundArgs {
+    const int32_t* begin; const int32_t* node_idx; const int32_t* r_begin; const int32_t* r_node_idx;
+    int32_t* color; int32_t* scc; uint8_t* mark;
+    unsigned long long* slot_key; int32_t* slot_pivot; int32_t* slot_fw; int32_t* slot_bw;
+    int64_t colour_cap;
+    int32_t* ctr;
+    const int32_t* live; int32_t live_count;
+    int32_t only_color;   // used when use_only
+    int32_t use_only;
+    const float* pivot_score;   // optional learned score per vertex (nullptr = degree rule)
+};
+
+__device__ __forceinline__ uint32_t pivot_hash(uint32_t v) {
+    uint32_t x = v * 0x9E3779B1u;
+    x ^= x >> 16; x *= 0x85EBCA6Bu; x ^= x >> 13;
+    return x;
+}
+
+// Pivot key: (min(in*out, 2^32-2)+1) << 32 | hash(v); never 0, unique per vertex.
+__device__ __forceinline__ unsigned long long pivot_key(const int32_t* __restrict__ begin,
+                                                        const int32_t* __restrict__ r_begin, int32_t v) {
+    unsigned long long outd = (unsigned)(__ldg(begin + v + 1) - __ldg(begin + v));
+    unsigned long long ind = (unsigned)(__ldg(r_begin + v + 1) - __ldg(r_begin + v));
+    unsigned long long prod = outd * ind;
+    if (prod > 0xFFFFFFFEull) prod = 0xFFFFFFFEull;
+    return ((prod + 1ull) << 32) | pivot_hash((uint32_t)v);
+}
+
+// Claim w for direction `dir` inside colour c; true if this thread claimed it.
+__device__ __forceinline__ bool visit(const RoundArgs& a, int32_t w, int32_t c, int dir) {
+    unsigned bit = 1u << dir;
+    if (*(volatile uint8_t*)(a.mark + w) & bit) return false;
+    if (__ldg(a.color + w) != c) return false;
+    unsigned sh = (unsigned)(w & 3) * 8u;
+    unsigned old = atomicOr(reinterpret_cast<unsigned*>(a.mark + (w & ~3)), bit << sh);
+    return ((old >> sh) & bit) == 0u;
+}
+
+int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen);

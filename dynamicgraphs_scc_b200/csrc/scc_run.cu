@@ -107,9 +107,13 @@ static int run_method(const scc_graph* g, scc_state* s, int method, scc_run_stat
     st->trimmed_second = t2;
     SCC_TRY(record(s, 3));
     if (s->live_count > 0 && method == SCC_METHOD_GLOBAL_WCC_FB) {
-        // WCC: do_global_wcc + create_work_items_from_wcc
-        SCC_TRY(scc_impl_wcc(g, s));
-        st->num_wcc_classes = s->h_ctr[CTR_NUM_CLASSES];
+        // WCC: colour the remainder into independent classes (create_work_items_from_wcc).
+        // The pipeline splits by weak components (union-find, a few passes whatever
+        // the diameter); the min-reach colouring of do_global_wcc is offered unchanged
+        // as scc_do_global_wcc.  Both give unions of SCCs, so the labels are the same.
+        int32_t classes = 0;
+        SCC_TRY(scc_impl_uf_split(g, s, &classes));
+        st->num_wcc_classes = classes;
     }
     SCC_TRY(record(s, 4));
     // FB: start_workers_fw_bw_dfs
@@ -135,6 +139,7 @@ extern "C" int scc_run(const scc_graph* g, scc_state* s, int method, int pivot_m
     st.pivot_mode = pivot_mode;
     int k0 = s->kernels;
     int64_t steps0 = s->traversal_steps;
+    int32_t rounds0 = s->fb_rounds;
     int rc = run_method(g, s, method, &st);
     if (rc != SCC_OK) return rc;
     SCC_CUDA(cudaStreamSynchronize(s->stream));
@@ -147,6 +152,7 @@ extern "C" int scc_run(const scc_graph* g, scc_state* s, int method, int pivot_m
     st.ms_total = elapsed(s, 0, 5);
     st.kernels_launched = s->kernels - k0;
     st.traversal_steps = s->traversal_steps - steps0;
+    st.fb_rounds = s->fb_rounds - rounds0;
     int32_t nscc = 0;
     SCC_TRY(scc_count_sccs(s, &nscc));
     st.num_sccs = nscc;

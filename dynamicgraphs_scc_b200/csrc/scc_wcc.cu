@@ -170,6 +170,119 @@ int scc_impl_wcc(const scc_graph* g, scc_state* s) {
     return SCC_OK;
 }
 
+// ------------------------------------------------------------------ weak-component split
+// Union-find over the live same-colour edges: every live vertex ends with
+// uf[v] = smallest vertex of its weakly connected component inside its colour.
+// Components are unions of SCCs, so they are valid independent classes, and
+// hooking converges in a few passes whatever the diameter (min-reach label
+// propagation above needs O(diameter) passes on grids and long cycles).
+__device__ __forceinline__ int32_t uf_find(int32_t* __restrict__ uf, int32_t x) {
+    int32_t p = __ldcg(uf + x);
+    while (p != x) {
+        int32_t gp = __ldcg(uf + p);
+        if (gp != p) uf[x] = gp;   // path halving; any ancestor is a valid parent
+        x = p;
+        p = gp;
+    }
+    return x;
+}
+
+__device__ __forceinline__ void uf_union(int32_t* __restrict__ uf, int32_t a, int32_t b) {
+    for (;;) {
+        a = uf_find(uf, a);
+        b = uf_find(uf, b);
+        if (a == b) return;
+        int32_t hi = max(a, b), lo = min(a, b);
+        if (atomicCAS(uf + hi, hi, lo) == hi) return;
+        a = hi; b = lo;
+    }
+}
+
+__global__ void k_uf_init(const int32_t* __restrict__ live, int32_t n_items, int32_t* __restrict__ uf) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_items; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t v = live[i];
+        uf[v] = v;
+    }
+}
+
+// One warp per 32 live vertices; high-degree vertices are walked by the whole warp.
+__global__ void k_uf_hook(const int32_t* __restrict__ begin, const int32_t* __restrict__ node_idx,
+                          const int32_t* __restrict__ live, int32_t n_items, const int32_t* __restrict__ color,
+                          int32_t* __restrict__ uf) {
+    int lane = threadIdx.x & 31;
+    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    int64_t groups = ((int64_t)n_items + 31) >> 5;
+    for (int64_t gi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; gi < groups; gi += nwarps) {
+        int64_t idx = gi * 32 + lane;
+        int32_t v = 0, b = 0, e = 0, c = SCC_COLOR_DONE;
+        if (idx < n_items) {
+            v = live[idx];
+            c = __ldg(color + v);
+            if (c != SCC_COLOR_DONE) { b = __ldg(begin + v); e = __ldg(begin + v + 1); }
+        }
+        int32_t deg = e - b;
+        unsigned big = __ballot_sync(0xFFFFFFFFu, deg > 32);
+        while (big) {
+            int l = __ffs(big) - 1;
+            big &= big - 1;
+            int32_t bv = __shfl_sync(0xFFFFFFFFu, v, l), bb = __shfl_sync(0xFFFFFFFFu, b, l);
+            int32_t be = __shfl_sync(0xFFFFFFFFu, e, l), bc = __shfl_sync(0xFFFFFFFFu, c, l);
+            for (int32_t k = bb + lane; k < be; k += 32) {
+                int32_t w = __ldg(node_idx + k);
+                if (w != bv && __ldg(color + w) == bc) uf_union(uf, bv, w);
+            }
+        }
+        if (deg <= 32) {
+            for (int32_t k = b; k < e; ++k) {
+                int32_t w = __ldg(node_idx + k);
+                if (w != v && __ldg(color + w) == c) uf_union(uf, v, w);
+            }
+        }
+    }
+}
+
+__global__ void k_uf_flatten(const int32_t* __restrict__ live, int32_t n_items, const int32_t* __restrict__ color,
+                             int32_t* __restrict__ uf, int32_t* __restrict__ label) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_items; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t v = live[i];
+        if (color[v] == SCC_COLOR_DONE) continue;
+        label[v] = uf_find(uf, v);
+    }
+}
+
+// Recolour every live vertex by its weak component: roots (uf == itself) take
+// colours 0..k-1 in ascending vertex order, members copy their root's colour.
+// The colour counter restarts at k-1: all earlier colours of live vertices are
+// overwritten, so colour ids stay below n.
+int scc_impl_uf_split(const scc_graph* g, scc_state* s, int32_t* num_classes) {
+    int32_t n_items = s->live_count;
+    *num_classes = 0;
+    if (n_items <= 0) return SCC_OK;
+    unsigned blocks = scc_blocks(n_items);
+    k_uf_init<<<blocks, SCC_THREADS, 0, s->stream>>>(s->live, n_items, s->uf);
+    SCC_LAUNCHED(s);
+    k_uf_hook<<<scc_blocks(n_items, SCC_THREADS, 148 * 16), SCC_THREADS, 0, s->stream>>>(
+        g->begin, g->node_idx, s->live, n_items, s->color, s->uf);
+    SCC_LAUNCHED(s);
+    k_uf_flatten<<<blocks, SCC_THREADS, 0, s->stream>>>(s->live, n_items, s->color, s->uf, s->wcc);
+    SCC_LAUNCHED(s);
+    int64_t tiles = ((int64_t)n_items + WCC_TILE - 1) / WCC_TILE;
+    k_root_count<<<(unsigned)tiles, SCC_THREADS, 0, s->stream>>>(s->live, n_items, s->color, s->wcc, s->block_sums);
+    SCC_LAUNCHED(s);
+    k_scan_tiles_wcc<<<1, 1024, 0, s->stream>>>((int32_t)tiles, s->block_sums, s->ctr + CTR_NUM_CLASSES);
+    SCC_LAUNCHED(s);
+    k_root_color<<<(unsigned)tiles, SCC_THREADS, 0, s->stream>>>(s->live, n_items, s->color, s->wcc, s->block_sums, 0);
+    SCC_LAUNCHED(s);
+    k_member_color<<<blocks, SCC_THREADS, 0, s->stream>>>(s->live, n_items, s->color, s->wcc);
+    SCC_LAUNCHED(s);
+    SCC_TRY(scc_sync_counters(s));
+    int32_t k = s->h_ctr[CTR_NUM_CLASSES];
+    int32_t last = k - 1;
+    SCC_CUDA(cudaMemcpyAsync(s->ctr + CTR_NEXT_COLOR, &last, sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
+    *num_classes = k;
+    return SCC_OK;
+}
+
 // ------------------------------------------------------------------ C ABI
 extern "C" int scc_do_global_wcc(const scc_graph* g, scc_state* s) {
     SCC_REQUIRE(g && s, SCC_ERR_INVALID, "NULL argument");
