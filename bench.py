@@ -37,17 +37,24 @@ WORKLOADS = {
     "c2": dict(rmat_scale=24, edge_factor=16, grid_side=4096, seed=2024),
     "rmat24": dict(rmat_scale=24, edge_factor=16, seed=2024),
     "c1": dict(rmat_scale=16, edge_factor=8, seed=42),
+    # smaller cases of the same shapes, for profiler captures
+    "rmat22": dict(rmat_scale=22, edge_factor=16, seed=2024),
+    "grid4096": dict(grid_side=4096, seed=2024),
 }
 # CPU-baseline sample of the same workload shape at 1/16 of the vertices
 CPU_SAMPLES = {
     "c2": dict(rmat_scale=20, edge_factor=16, grid_side=1024, seed=2024),
     "rmat24": dict(rmat_scale=20, edge_factor=16, seed=2024),
     "c1": dict(rmat_scale=16, edge_factor=8, seed=42),
+    "rmat22": dict(rmat_scale=18, edge_factor=16, seed=2024),
+    "grid4096": dict(grid_side=1024, seed=2024),
 }
 WORKLOAD_NAMES = {
     "c2": "R-MAT s24 ef16 (a=.57,b=.19,c=.19) U 4096x4096 randomly oriented grid (+5% bidirectional)",
     "rmat24": "R-MAT s24 ef16 (a=.57,b=.19,c=.19)",
     "c1": "R-MAT s16 ef8 (a=.57,b=.19,c=.19)",
+    "rmat22": "R-MAT s22 ef16 (a=.57,b=.19,c=.19)",
+    "grid4096": "4096x4096 randomly oriented grid (+5% bidirectional)",
 }
 
 
@@ -61,58 +68,61 @@ def measured_peak_gbs():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event reasons sampled (NVML, every 10 ms) during the timed region.
+    Reads only; changes no GPU setting."""
 
-    def __init__(self, index: int):
-        self.index = index
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, torch_device: int):
+        self.dev = torch_device
         self.samples = []
-        self.proc = None
+        self.reasons = set()
+        self.max_mhz = None
+        self.stop_flag = threading.Event()
         self.thread = None
+        self.handle = None
+
+    def _open(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.dev)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
 
     def start(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.nvml, self.handle = self._open()
+            self.max_mhz = self.nvml.nvmlDeviceGetMaxClockInfo(self.handle, self.nvml.NVML_CLOCK_SM)
         except Exception:
-            self.proc = None
+            self.handle = None
             return
-        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread = threading.Thread(target=self._run, daemon=True)
         self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                self.samples.append(parts)
+    def _run(self):
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append(self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM))
+                mask = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                for bit, name in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.01)
 
     def stop(self):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self.stop_flag.set()
         if self.thread is not None:
             self.thread.join(timeout=2)
-        sm = []
-        mx = None
-        reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for p in self.samples:
-            try:
-                sm.append(float(p[1]))
-                mx = float(p[2])
-            except ValueError:
-                continue
-            for nm, val in zip(names, p[5:9]):
-                if val.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = self.samples
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(sm)}
 
 
 def run_reference(args, workload):
@@ -121,7 +131,7 @@ def run_reference(args, workload):
     from dynamicgraphs_scc_b200 import generate_edges_host
     kw = CPU_SAMPLES[workload]
     n, s, d = generate_edges_host(**kw)
-    s, d = O.dedup_edges(s, d)
+    s, d = O.dedup_edges(s, d, n=n)
     csr = O.build_csr(n, s, d)
     threads = os.cpu_count() or 1
     kind = "reference" if O.ref_available() else "port"
@@ -238,7 +248,7 @@ def main():
     labels = torch.empty(n, dtype=torch.int32).pin_memory()
     lib = capi.lib()
     e2e_ms = []
-    for i in range(args.e2e_steps + 1):
+    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -253,12 +263,12 @@ def main():
         st.synchronize()
         if i > 0:
             e2e_ms.append(e0.elapsed_time(e1))
-    e2e = statistics.mean(e2e_ms)
+    e2e = statistics.mean(e2e_ms) if e2e_ms else float("nan")
     if dist is not None:
         t = torch.tensor([e2e], device=f"cuda:{local_rank}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e = float(t.item())
-    e2e_gteps = total_edges / (e2e * 1e-3) / 1e9
+    e2e_gteps = total_edges / (e2e * 1e-3) / 1e9 if e2e_ms else None
     h2d = 4 * (2 * (n + 1) + 2 * m)
     d2h = 4 * n
 
@@ -287,7 +297,8 @@ def main():
         "roofline": {"bound": "hbm", "scope": "whole step (16M+20N+8 algorithmic bytes)",
                      "achieved": round(achieved, 2), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(achieved / peak, 5), "traffic": None},
-        "e2e": {"value": round(e2e_gteps, 4), "unit": "GTEPS", "ms_per_step": round(e2e, 3),
+        "e2e": {"value": round(e2e_gteps, 4) if e2e_gteps else None, "unit": "GTEPS",
+                "ms_per_step": round(e2e, 3) if e2e_ms else None,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "cpu_baseline": cpu,
         "clocks": clocks,

@@ -126,6 +126,7 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
                       int32_t* scc_found, int32_t* active) {
     *scc_found = 0;
     if (active) *active = 0;
+    s->fresh = false;
     if (s->live_count <= 0) return SCC_OK;
     SCC_TRY(scc_sync_counters(s));
     SCC_TRY(scc_impl_ensure_colour_cap(s, (int64_t)s->h_ctr[CTR_NEXT_COLOR] + 2LL * s->live_count + 1024));

@@ -80,6 +80,7 @@ struct scc_state {
     int kernels = 0;                 // kernels launched (statistics)
     int64_t traversal_steps = 0;
     int32_t fb_rounds = 0;           // recursion rounds (statistics)
+    bool fresh = false;              // colours all -1 and nothing finished (set by reset, cleared by any phase)
 
     int32_t* color = nullptr;        // G_Color [n]
     int32_t* scc = nullptr;          // G_SCC   [n]

@@ -121,6 +121,39 @@ __global__ void k_trim1_sweep(TrimArgs a, const int32_t* __restrict__ list, int6
     block_count_add(a.ctr + CTR_COUNT, cnt);
 }
 
+// First sweep on a fresh state (every colour -1, nothing finished): v starts
+// trimmable exactly when one of its sorted adjacency lists is empty or holds
+// only v itself (self-loops do not count), which the offsets and the first and
+// last entries decide without reading any colour.  Later peels cascade with
+// the full colour test.
+__device__ __forceinline__ bool has_other_nbr_sorted(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                                     int32_t v) {
+    int32_t b = __ldg(off + v), e = __ldg(off + v + 1);
+    if (b == e) return false;
+    return __ldg(adj + b) != v || __ldg(adj + e - 1) != v;
+}
+
+__global__ void k_trim1_fresh(TrimArgs a, int32_t n) {
+    scc_graph g = as_graph(a);
+    int32_t cnt = 0;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t limit = (((int64_t)n + 31) / 32) * 32;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += stride) {
+        if (i < n) {
+            int32_t v = (int32_t)i;
+            if (!has_other_nbr_sorted(a.begin, a.node_idx, v) || !has_other_nbr_sorted(a.r_begin, a.r_node_idx, v)) {
+                if (atomicCAS(a.color + v, SCC_COLOR_INIT, SCC_COLOR_DONE) == SCC_COLOR_INIT) {
+                    a.scc[v] = v;
+                    __threadfence();
+                    cnt++;
+                    cascade(a, g, v, SCC_COLOR_INIT, cnt);
+                }
+            }
+        }
+    }
+    block_count_add(a.ctr + CTR_COUNT, cnt);
+}
+
 // Overflow expansion: one warp per already-trimmed vertex x, lanes stride its
 // neighbours; newly trimmed neighbours cascade per lane.
 __global__ void k_trim1_overflow(TrimArgs a, const int32_t* __restrict__ items, int32_t n_items,
@@ -154,6 +187,11 @@ __global__ void k_save_colors(const int32_t* __restrict__ items, int32_t n, cons
         out[i] = saved_src[items[i]];
 }
 
+__global__ void k_fill_aux(int64_t n, int32_t* __restrict__ b, int32_t v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = v;
+}
+
 // Colour snapshot used to recover the colour a vertex had before it was trimmed.
 __global__ void k_copy_i32(int64_t n, const int32_t* __restrict__ a, int32_t* __restrict__ b) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -174,10 +212,15 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
     *trimmed = 0;
     if (n_items <= 0) return SCC_OK;
     // snapshot colours (aux) so overflowed vertices keep their pre-trim colour
-    if (use_live)
+    bool fresh = s->fresh && !use_live;
+    if (fresh) {
+        // every colour is -1: the snapshot the overflow path reads is that constant
+        k_fill_aux<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(n_items, s->aux, SCC_COLOR_INIT);
+    } else if (use_live) {
         k_copy_list_i32<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(list, n_items, s->color, s->aux);
-    else
+    } else {
         k_copy_i32<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(n_items, s->color, s->aux);
+    }
     SCC_LAUNCHED(s);
     TrimArgs a;
     a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin; a.r_node_idx = g->r_node_idx;
@@ -185,8 +228,12 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
     a.ovf = s->qa;
     SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
     SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
-    k_trim1_sweep<<<scc_blocks(n_items, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, list, n_items);
+    if (fresh)
+        k_trim1_fresh<<<scc_blocks(n_items, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, (int32_t)n_items);
+    else
+        k_trim1_sweep<<<scc_blocks(n_items, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, list, n_items);
     SCC_LAUNCHED(s);
+    s->fresh = false;
     int64_t total = 0;
     for (int round = 0; round < 1000000; ++round) {
         SCC_TRY(scc_sync_counters(s));
@@ -266,6 +313,7 @@ __global__ void k_trim2_apply(int32_t* __restrict__ color, int32_t* __restrict__
 
 int scc_impl_trim2(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     *trimmed = 0;
+    s->fresh = false;
     bool use_live = s->live_count >= 0;
     int64_t n_items = use_live ? s->live_count : g->n;
     const int32_t* list = use_live ? s->live : nullptr;

@@ -35,6 +35,8 @@ def lib():
         L = C.CDLL(ORACLE_SO)
         L.orc_build_csr.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P, _I32P, _I32P, _I32P, _I32P]
         L.orc_build_csr.restype = None
+        L.orc_dedup_edges.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P]
+        L.orc_dedup_edges.restype = C.c_int64
         L.orc_tarjan.argtypes = [C.c_int32, _I32P, _I32P, _I32P]
         L.orc_tarjan.restype = None
         L.orc_canonical.argtypes = [C.c_int32, _I32P, _I32P]
@@ -76,8 +78,14 @@ def ref():
 
 
 # ------------------------------------------------------------------------ graph helpers
-def dedup_edges(src, dst, drop_self_loops=True):
-    """Remove self-loops and duplicate (src, dst) pairs (the generators' post-processing)."""
+def dedup_edges(src, dst, drop_self_loops=True, n=None):
+    """Remove self-loops and duplicate (src, dst) pairs (the generators' post-processing),
+    returned sorted by (src, dst)."""
+    if drop_self_loops and n is not None:
+        s = np.array(src, np.int32, copy=True)
+        d = np.array(dst, np.int32, copy=True)
+        k = lib().orc_dedup_edges(n, s.size, _p(s), _p(d))
+        return s[:k].copy(), d[:k].copy()
     s = np.asarray(src, np.int64)
     d = np.asarray(dst, np.int64)
     if drop_self_loops:
@@ -143,14 +151,38 @@ def fw_bw(csr, color, scc, base, pivot, fw_color, bw_color):
     return int(s), f.value, w.value
 
 
-def ref_method2(csr, threads=None, pin=False):
+class _QuietStdout:
+    """Send the reference's own printf output (it announces each method on stdout)
+    to /dev/null, flushing C stdio before the descriptor is restored."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        C.CDLL(None).fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+        return False
+
+
+def ref_method2(csr, threads=None, pin=False, quiet=True):
     """The reference's own method-2 pipeline: (canonical labels, run ms)."""
     b, a = csr[0], csr[1]
     n = b.size - 1
     out = np.empty(max(n, 1), np.int32)
     ms = C.c_double()
     th = threads or os.cpu_count() or 1
-    rc = ref().ref_method2(n, a.size, _p(b), _p(a), th, int(pin), _p(out), C.byref(ms))
+    if quiet:
+        with _QuietStdout():
+            rc = ref().ref_method2(n, a.size, _p(b), _p(a), th, int(pin), _p(out), C.byref(ms))
+    else:
+        rc = ref().ref_method2(n, a.size, _p(b), _p(a), th, int(pin), _p(out), C.byref(ms))
     if rc != 0:
         raise RuntimeError("reference method 2 failed")
     return canonical(out[:n]), ms.value

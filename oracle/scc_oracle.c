@@ -34,25 +34,50 @@ static int cmp_i32(const void* a, const void* b) {
     return (x > y) - (x < y);
 }
 
+/* One side: rows = key, columns = val, each row sorted.  Two stable counting
+ * passes (by val, then by key) give rows already sorted, no comparison sort. */
+static void csr_side(int32_t n, int64_t m, const int32_t* key, const int32_t* val, int32_t* off, int32_t* out) {
+    int32_t* cnt = (int32_t*)calloc((size_t)n + 1, sizeof(int32_t));
+    int64_t* tmp_pos = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m > 0 ? m : 1));
+    int64_t* order = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m > 0 ? m : 1));
+    int64_t* vstart = (int64_t*)calloc((size_t)n + 1, sizeof(int64_t));
+    for (int64_t e = 0; e < m; ++e) vstart[val[e] + 1]++;
+    for (int32_t v = 0; v < n; ++v) vstart[v + 1] += vstart[v];
+    for (int64_t e = 0; e < m; ++e) tmp_pos[vstart[val[e]]++] = e;   /* edges ordered by val */
+    memset(off, 0, sizeof(int32_t) * ((size_t)n + 1));
+    for (int64_t e = 0; e < m; ++e) off[key[e] + 1]++;
+    for (int32_t v = 0; v < n; ++v) off[v + 1] += off[v];
+    memcpy(cnt, off, sizeof(int32_t) * ((size_t)n + 1));
+    for (int64_t i = 0; i < m; ++i) { int64_t e = tmp_pos[i]; order[cnt[key[e]]++] = e; }
+    for (int64_t i = 0; i < m; ++i) out[i] = val[order[i]];
+    free(cnt); free(tmp_pos); free(order); free(vstart);
+}
+
 void orc_build_csr(int32_t n, int64_t m, const int32_t* src, const int32_t* dst,
                    int32_t* begin, int32_t* node_idx, int32_t* r_begin, int32_t* r_node_idx) {
-    memset(begin, 0, sizeof(int32_t) * (size_t)(n + 1));
-    memset(r_begin, 0, sizeof(int32_t) * (size_t)(n + 1));
-    for (int64_t e = 0; e < m; ++e) { begin[src[e] + 1]++; r_begin[dst[e] + 1]++; }
-    for (int32_t v = 0; v < n; ++v) { begin[v + 1] += begin[v]; r_begin[v + 1] += r_begin[v]; }
-    int32_t* fill = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n + 1));
-    int32_t* rfill = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n + 1));
-    memcpy(fill, begin, sizeof(int32_t) * (size_t)(n + 1));
-    memcpy(rfill, r_begin, sizeof(int32_t) * (size_t)(n + 1));
-    for (int64_t e = 0; e < m; ++e) {
-        node_idx[fill[src[e]]++] = dst[e];
-        r_node_idx[rfill[dst[e]]++] = src[e];
-    }
+    csr_side(n, m, src, dst, begin, node_idx);
+    csr_side(n, m, dst, src, r_begin, r_node_idx);
+}
+
+/* Generator post-processing: drop self-loops and duplicate edges (in place),
+ * returning the new edge count.  Sorting by (src, dst) via csr_side. */
+int64_t orc_dedup_edges(int32_t n, int64_t m, int32_t* src, int32_t* dst) {
+    int32_t* off = (int32_t*)malloc(sizeof(int32_t) * ((size_t)n + 1));
+    int32_t* adj = (int32_t*)malloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+    csr_side(n, m, src, dst, off, adj);
+    int64_t k = 0;
     for (int32_t v = 0; v < n; ++v) {
-        qsort(node_idx + begin[v], (size_t)(begin[v + 1] - begin[v]), sizeof(int32_t), cmp_i32);
-        qsort(r_node_idx + r_begin[v], (size_t)(r_begin[v + 1] - r_begin[v]), sizeof(int32_t), cmp_i32);
+        int32_t prev = -1;
+        for (int32_t i = off[v]; i < off[v + 1]; ++i) {
+            int32_t w = adj[i];
+            if (w == v || w == prev) continue;
+            prev = w;
+            src[k] = v; dst[k] = w; k++;
+        }
     }
-    free(fill); free(rfill);
+    free(off); free(adj);
+    (void)cmp_i32;
+    return k;
 }
 
 /* ------------------------------------------------------------------------ */

@@ -75,7 +75,7 @@ def main() -> None:
     meta = []
     for name, kw in GEN_CASES:
         n, s, d = generate_edges_host(**kw)
-        s, d = O.dedup_edges(s, d)
+        s, d = O.dedup_edges(s, d, n=n)
         csr = O.build_csr(n, s, d)
         m2, _ = O.ref_method2(csr)
         tj, _ = O.ref_tarjan(csr)

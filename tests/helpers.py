@@ -28,7 +28,7 @@ def golden_cases():
         name = c["name"]
         if c["kind"] == "gen":
             n, s, d = generate_edges_host(**c["params"])
-            s, d = O.dedup_edges(s, d)
+            s, d = O.dedup_edges(s, d, n=n)
         else:
             n, s, d = c["n"], z[f"{name}__src"], z[f"{name}__dst"]
         out.append(dict(name=name, n=n, src=np.asarray(s, np.int32), dst=np.asarray(d, np.int32),
@@ -39,7 +39,7 @@ def golden_cases():
 def seeded_graph(**kw):
     """Deduplicated seeded edge list and its oracle CSR."""
     n, s, d = generate_edges_host(**kw)
-    s, d = O.dedup_edges(s, d)
+    s, d = O.dedup_edges(s, d, n=n)
     return n, s, d, O.build_csr(n, s, d)
 
 
