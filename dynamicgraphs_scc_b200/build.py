@@ -29,6 +29,7 @@ CU_SOURCES = [
     "scc_wcc.cu",
     "scc_run.cu",
     "scc_gen.cu",
+    "scc_noalloc.cu",
 ]
 
 

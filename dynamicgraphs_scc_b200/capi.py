@@ -96,6 +96,7 @@ _SIGS = {
     "scc_repeat_global_trim1": [_P, _P, C.c_int32, _I32P],
     "scc_repeat_global_trim1_compact": [_P, _P, C.c_int32, _I32P],
     "scc_create_trim1_compact": [_P, _P, _I32P],
+    "scc_trim1_noalloc": [C.c_int32, _P, _P, _P, _P, _P, _P, _I32P, _P],
     "scc_do_global_trim2_new": [_P, _P, _I32P],
     "scc_do_global_trim2": [_P, _P, _I32P],
     "scc_repeat_global_trim2_new": [_P, _P, C.c_int32, _I32P],

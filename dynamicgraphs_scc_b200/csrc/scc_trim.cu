@@ -254,6 +254,46 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
     return SCC_OK;
 }
 
+// Trim1 to the fixpoint over all n vertices of caller-owned arrays, with every
+// scratch buffer supplied by the caller (snapshot, two overflow lists and the
+// overflow items' colours: n ints each; ctr: CTR_MAX ints).  Same kernels and
+// sweep as scc_do_global_trim1; used by the allocation-free entry point.
+int scc_trim1_with_scratch(int32_t n, const int32_t* begin, const int32_t* node_idx, const int32_t* r_begin,
+                           const int32_t* r_node_idx, int32_t* color, int32_t* scc, int32_t* snapshot,
+                           int32_t* ovf_a, int32_t* ovf_b, int32_t* item_colors, int32_t* ctr, cudaStream_t st,
+                           int32_t* trimmed) {
+    *trimmed = 0;
+    if (n <= 0) return SCC_OK;
+    int32_t h_ctr[CTR_MAX];
+    k_copy_i32<<<scc_blocks(n), SCC_THREADS, 0, st>>>(n, color, snapshot);
+    SCC_CUDA(cudaPeekAtLastError());
+    TrimArgs a;
+    a.begin = begin; a.node_idx = node_idx; a.r_begin = r_begin; a.r_node_idx = r_node_idx;
+    a.color = color; a.scc = scc; a.ctr = ctr;
+    a.ovf = ovf_a;
+    SCC_CUDA(cudaMemsetAsync(ctr, 0, sizeof(int32_t) * CTR_MAX, st));
+    k_trim1_sweep<<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, st>>>(a, nullptr, n);
+    SCC_CUDA(cudaPeekAtLastError());
+    int64_t total = 0;
+    for (int round = 0; round < 1000000; ++round) {
+        SCC_CUDA(cudaMemcpyAsync(h_ctr, ctr, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
+        SCC_CUDA(cudaStreamSynchronize(st));
+        total += h_ctr[CTR_COUNT];
+        int32_t novf = h_ctr[CTR_OVERFLOW];
+        if (novf == 0) break;
+        SCC_CUDA(cudaMemcpyAsync(ovf_b, ovf_a, sizeof(int32_t) * (size_t)novf, cudaMemcpyDeviceToDevice, st));
+        k_save_colors<<<scc_blocks(novf), SCC_THREADS, 0, st>>>(ovf_b, novf, snapshot, item_colors);
+        SCC_CUDA(cudaPeekAtLastError());
+        SCC_CUDA(cudaMemsetAsync(ctr + CTR_COUNT, 0, sizeof(int32_t), st));
+        SCC_CUDA(cudaMemsetAsync(ctr + CTR_OVERFLOW, 0, sizeof(int32_t), st));
+        k_trim1_overflow<<<scc_blocks((int64_t)novf * 32, SCC_THREADS, 148 * 8), SCC_THREADS, 0, st>>>(
+            a, ovf_b, novf, item_colors);
+        SCC_CUDA(cudaPeekAtLastError());
+    }
+    *trimmed = (int32_t)total;
+    return SCC_OK;
+}
+
 // ------------------------------------------------------------------ trim2
 __device__ __forceinline__ bool degree_is_one(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                                               const int32_t* __restrict__ color, int32_t c, int32_t v, int32_t* nbr) {

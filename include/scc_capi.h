@@ -151,6 +151,26 @@ int scc_repeat_global_trim1_compact(const scc_graph* g, scc_state* s, int32_t tr
 /* create_trim1_compact (scc_trim1.cc:266-275): live vertices (colour != -2), ascending. */
 int scc_create_trim1_compact(const scc_graph* g, scc_state* s, int32_t* live_count);
 
+/* Trim1 with no device allocation.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc: a serving process that reserves
+ * its device-memory budget at start-up and must not fail or stall on an
+ * allocation mid-request, or a host that lends the library a fixed pool.
+ * Same result as scc_do_global_trim1 (peel to the fixpoint inside each
+ * colour) on caller-owned device arrays of the current device: the CSR and
+ * transpose (n+1 / m ints), d_color and d_scc (n ints, updated in place).
+ * The scratch lives in one file-scope __device__ array of
+ * 4 * SCC_NOALLOC_MAX_NODES + 128 ints (about 16 MiB) that every GPU loading
+ * the library holds until exit; n above SCC_NOALLOC_MAX_NODES is rejected with
+ * SCC_ERR_INVALID.  The first call on a device looks up that array's device
+ * address (make that first call before any stream capture).  All calls share
+ * the array, so calls that overlap on the GPU (other streams, other host
+ * threads) race; serialise them.  Work is ordered on `stream` (cudaStream_t as
+ * void*, NULL = legacy default stream) and the call returns once it is done. */
+#define SCC_NOALLOC_MAX_NODES (1 << 20)
+int scc_trim1_noalloc(int32_t n, const int32_t* d_begin, const int32_t* d_node_idx,
+                      const int32_t* d_r_begin, const int32_t* d_r_node_idx,
+                      int32_t* d_color, int32_t* d_scc, int32_t* trimmed, void* stream);
+
 /* ---- trim2 (src/scc_trim2_new.cc, src/scc_trim2.cc) ---------------------------------- */
 /* do_global_trim2_new (scc_trim2_new.cc:80-102): 2-vertex SCCs among the compact
  * targets, decided on the colours as they stood before the pass. */
