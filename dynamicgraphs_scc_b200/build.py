@@ -30,6 +30,7 @@ CU_SOURCES = [
     "scc_run.cu",
     "scc_gen.cu",
     "scc_noalloc.cu",
+    "scc_update.cu",
 ]
 
 

@@ -45,6 +45,17 @@ class RunStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class UpdateStats(C.Structure):
+    _fields_ = [
+        ("ms_total", C.c_double), ("ms_merge", C.c_double), ("ms_delete", C.c_double), ("ms_insert", C.c_double),
+        ("affected_delete", C.c_int32), ("affected_insert", C.c_int32), ("m_after", C.c_int64),
+        ("num_sccs", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class GenParams(C.Structure):
     _fields_ = [
         ("rmat_scale", C.c_int), ("edge_factor", C.c_int), ("grid_side", C.c_int), ("num_cycles", C.c_int),
@@ -87,6 +98,8 @@ _SIGS = {
     "scc_state_get_wcc": [_P, _I32P],
     "scc_state_get_trim_targets": [_P, _I32P, C.c_int32, _I32P],
     "scc_state_device_arrays": [_P, C.POINTER(_P), C.POINTER(_P)],
+    "scc_state_profile": [_P, C.c_int],
+    "scc_state_profile_read": [_P, C.POINTER(C.c_double), _I64P, _I64P, _I64P],
     "scc_get_new_color": [_P, _I32P],
     "scc_get_curr_color": [_P, _I32P],
     "scc_choose_pivot_from_color": [_P, _P, C.c_int32, _I32P],
@@ -118,6 +131,11 @@ _SIGS = {
     "scc_histogram": [_P, _I32P, _I32P, C.c_int32, _I32P],
     "scc_decompose_csr": [C.c_int32, C.c_int32, _I32P, _I32P, _I32P, _I32P, C.c_int, C.c_int, _I32P, _I32P,
                           C.POINTER(RunStats)],
+    "scc_update_batch": [_P, _P, C.c_int64, _P, _P, C.c_int64, _P, _P, C.c_int, C.POINTER(UpdateStats)],
+    "scc_incremental_insert": [_P, _P, C.c_int64, _I32P, _I32P, C.POINTER(UpdateStats)],
+    "scc_decremental_delete": [_P, _P, C.c_int64, _I32P, _I32P, C.POINTER(UpdateStats)],
+    "scc_insert_idea1": [_P, _P, C.c_int64, _I32P, _I32P, C.POINTER(RunStats)],
+    "scc_condensation_graph": [_P, _I32P, C.c_int32, C.c_int64, _I32P, _I32P, C.POINTER(_P)],
     "scc_gen_sizes": [C.POINTER(GenParams), _I32P, _I64P],
     "scc_gen_edges_host": [C.POINTER(GenParams), _I32P, _I32P, C.c_int64, _I64P],
     "scc_gen_graph": [C.POINTER(GenParams), C.c_int, C.c_int, C.POINTER(_P)],

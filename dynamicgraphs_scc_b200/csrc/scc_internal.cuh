@@ -61,6 +61,8 @@ enum {
     CTR_SPARE4,
     CTR_EDGES = 16,      // u64 (slots 16-17): edges of the next top-down frontier
     CTR_LIVE_EDGES = 18, // u64 (slots 18-19): in+out degree of the vertices being traversed
+    CTR_ASYNC_ITEMS = 20,// u64 (slots 20-21): items expanded by the asynchronous drain (ledger)
+    CTR_ASYNC_EDGES = 22,// u64 (slots 22-23): edges scanned by it
     // asynchronous traversal queue counters, one 128-byte line each (polled by idle warps)
     CTR_AHEAD = 32,
     CTR_ATAIL = 64,
@@ -92,6 +94,8 @@ struct scc_state {
     int32_t* qb = nullptr;           // [2n+64] traversal queue B
     int32_t* aq = nullptr;           // [2n+64] asynchronous traversal queue, kept at -1 between uses
     int32_t* uf = nullptr;           // [n] union-find parents (weak-component split)
+    int32_t* cnt_out = nullptr;      // [n] live out-neighbour counts (counting peel on a fresh state)
+    int32_t* cnt_in = nullptr;       // [n] live in-neighbour counts
     int32_t* hq = nullptr;           // [2n+64] high-degree items deferred by a top-down level
     long long* hoff = nullptr;       // [2n+64] prefix of their degrees
     uint8_t* mark = nullptr;         // [n rounded to 4] reachability marks (bit0 FW, bit1 BW)
@@ -117,6 +121,15 @@ struct scc_state {
 
     cudaEvent_t ev[16];
     bool events = false;
+
+    // kernel ledger (scc_state_profile): device time and algorithmic bytes of
+    // the asynchronous reachability drain, timed with events on `stream`
+    bool ledger_on = false;
+    cudaEvent_t lev[2];
+    double ledger_ms = 0.0;
+    long long ledger_launches = 0;
+    long long ledger_items = 0;
+    long long ledger_edges = 0;
 };
 
 // ---------------------------------------------------------------- helpers (host)

@@ -41,7 +41,8 @@
 #define HUGE_DEG 4096
 template <class Push>
 __device__ __forceinline__ void expand_warp(const RoundArgs& a, bool valid, int32_t it, Push& push,
-                                            int32_t* huge_list = nullptr, int32_t* huge_cnt = nullptr) {
+                                            int32_t* huge_list = nullptr, int32_t* huge_cnt = nullptr,
+                                            long long* edge_acc = nullptr) {
     int lane = threadIdx.x & 31;
     int32_t v = 0, dir = 0, b = 0, e = 0, c = 0;
     if (valid) {
@@ -51,6 +52,7 @@ __device__ __forceinline__ void expand_warp(const RoundArgs& a, bool valid, int3
         b = __ldg(off + v);
         e = __ldg(off + v + 1);
         c = __ldg(a.color + v);
+        if (edge_acc) *edge_acc += e - b;
         if (huge_list && e - b > HUGE_DEG) {
             huge_list[atomicAdd(huge_cnt, 1)] = it;
             e = b;
@@ -276,7 +278,9 @@ __global__ void __launch_bounds__(REACH_THREADS) k_reach_bottomup(RoundArgs a, i
 
 // ------------------------------------------------------------------ asynchronous mode
 struct LocalPush {
-    int32_t* buf;          // warp's shared list
+    int32_t* buf;          // warp's shared list: items
+    int32_t* bb;           //   and their adjacency range [bb, be) in the item's direction
+    int32_t* be;
     int32_t count;         // warp-uniform
     int32_t pushed;        // items added since the last work-counter update
     int32_t* q; int32_t* tail; int32_t* work; int64_t qcap; int32_t* err;
@@ -299,10 +303,14 @@ struct LocalPush {
         }
         __syncwarp();
     }
-    __device__ __forceinline__ void operator()(bool p, int32_t item) {
+    // Items spilled to the global queue lose their range (the taker reloads it).
+    __device__ __forceinline__ void operator()(bool p, int32_t item, int32_t b, int32_t e) {
         int lane = threadIdx.x & 31;
         unsigned bal = __ballot_sync(0xFFFFFFFFu, p);
-        if (p) buf[count + __popc(bal & ((1u << lane) - 1u))] = item;
+        if (p) {
+            int32_t pos = count + __popc(bal & ((1u << lane) - 1u));
+            buf[pos] = item; bb[pos] = b; be[pos] = e;
+        }
         int32_t k = __popc(bal);
         count += k;
         pushed += k;
@@ -310,18 +318,98 @@ struct LocalPush {
     }
 };
 
+// Asynchronous-mode expansion.  Each item arrives with its adjacency range
+// when it was claimed locally (b < 0 when it came through the global queue);
+// a claim loads the claimed vertex's range in the same round trip as the
+// atomic, so the next hop starts at the adjacency read.
+__device__ __forceinline__ void expand_warp_async(const RoundArgs& a, bool valid, int32_t it, int32_t b, int32_t e,
+                                                  LocalPush& push, long long* edge_acc) {
+    int lane = threadIdx.x & 31;
+    int32_t dir = 0, c = 0;
+    if (valid) {
+        int32_t v = it & ITEM_MASK;
+        dir = (it >> DIR_SHIFT) & 1;
+        const int32_t* off = dir ? a.r_begin : a.begin;
+        if (b < 0) { b = __ldg(off + v); e = __ldg(off + v + 1); }
+        c = __ldg(a.color + v);
+        *edge_acc += e - b;
+    } else {
+        b = e = 0;
+    }
+    int32_t deg = e - b;
+    unsigned big = __ballot_sync(0xFFFFFFFFu, deg > 32);
+    while (big) {
+        int l = __ffs(big) - 1;
+        big &= big - 1;
+        int32_t lb = __shfl_sync(0xFFFFFFFFu, b, l), le = __shfl_sync(0xFFFFFFFFu, e, l);
+        int32_t lc = __shfl_sync(0xFFFFFFFFu, c, l), ld = __shfl_sync(0xFFFFFFFFu, dir, l);
+        const int32_t* adj = ld ? a.r_node_idx : a.node_idx;
+        const int32_t* off = ld ? a.r_begin : a.begin;
+        for (int32_t k0 = lb; k0 < le; k0 += 32) {
+            int32_t k = k0 + lane;
+            bool p = false;
+            int32_t w = 0, wb = -1, we = -1;
+            if (k < le) {
+                w = __ldg(adj + k);
+                p = visit(a, w, lc, ld);
+                if (p) { wb = __ldg(off + w); we = __ldg(off + w + 1); }
+            }
+            push(p, w | (ld << DIR_SHIFT), wb, we);
+        }
+    }
+    int32_t mydeg = deg <= 32 ? deg : 0;
+    int32_t maxd = (int32_t)__reduce_max_sync(0xFFFFFFFFu, (unsigned)mydeg);
+    const int32_t* adj = dir ? a.r_node_idx : a.node_idx;
+    const int32_t* off = dir ? a.r_begin : a.begin;
+    const unsigned bit = 1u << dir;
+    for (int32_t j0 = 0; j0 < maxd; j0 += 4) {
+        int32_t w[4], wb[4], we[4];
+        bool p[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            p[u] = (j0 + u) < mydeg;
+            w[u] = p[u] ? __ldg(adj + b + j0 + u) : 0;
+        }
+        unsigned mk[4];
+        int32_t col[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            mk[u] = p[u] ? (unsigned)*(volatile uint8_t*)(a.mark + w[u]) : bit;
+            col[u] = p[u] ? __ldg(a.color + w[u]) : c;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            p[u] = p[u] && !(mk[u] & bit) && col[u] == c;
+            wb[u] = we[u] = -1;
+            if (p[u]) {
+                unsigned sh = (unsigned)(w[u] & 3) * 8u;
+                unsigned old = atomicOr(reinterpret_cast<unsigned*>(a.mark + (w[u] & ~3)), bit << sh);
+                wb[u] = __ldg(off + w[u]);
+                we[u] = __ldg(off + w[u] + 1);
+                p[u] = ((old >> sh) & bit) == 0u;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) push(p[u], w[u] | (dir << DIR_SHIFT), wb[u], we[u]);
+    }
+}
+
 __device__ __forceinline__ int32_t ld_volatile(const int32_t* p) { return *(const volatile int32_t*)p; }
 
 __global__ void __launch_bounds__(REACH_THREADS) k_reach_async(RoundArgs a, int32_t* __restrict__ q, int64_t qcap) {
     __shared__ int32_t sbuf[REACH_THREADS / 32][WBUF];
+    __shared__ int32_t sbeg[REACH_THREADS / 32][WBUF];
+    __shared__ int32_t send[REACH_THREADS / 32][WBUF];
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int32_t* head = a.ctr + CTR_AHEAD;
     int32_t* tail = a.ctr + CTR_ATAIL;
     int32_t* work = a.ctr + CTR_AWORK;
     int32_t* err = a.ctr + CTR_ERROR;
-    LocalPush push{sbuf[wid], 0, 0, q, tail, work, qcap, err};
+    LocalPush push{sbuf[wid], sbeg[wid], send[wid], 0, 0, q, tail, work, qcap, err};
     int idle = 0;
     int32_t last_work = -1;
+    long long my_edges = 0;     // per lane
+    long long my_items = 0;     // warp-uniform
     while (true) {
         if (push.count == 0) {
             int32_t got = 0, base = 0;
@@ -364,20 +452,30 @@ __global__ void __launch_bounds__(REACH_THREADS) k_reach_async(RoundArgs a, int3
                 if (lane == 0) { atomicExch(err, SCC_DEVERR_WAIT_LIMIT); atomicExch(a.ctr + CTR_ERROR_INFO, 2); }
                 break;
             }
-            if (lane < got) push.buf[lane] = item;
+            if (lane < got) { push.buf[lane] = item; push.bb[lane] = -1; push.be[lane] = -1; }
             __syncwarp();
             push.count = got;
         }
         int32_t k = min(32, push.count);
-        int32_t it = (lane < k) ? push.buf[push.count - k + lane] : 0;
+        int32_t top = push.count - k + lane;
+        int32_t it = (lane < k) ? push.buf[top] : 0;
+        int32_t ib = (lane < k) ? push.bb[top] : 0;
+        int32_t ie = (lane < k) ? push.be[top] : 0;
         __syncwarp();
         push.count -= k;
-        expand_warp(a, lane < k, it, push);
+        expand_warp_async(a, lane < k, it, ib, ie, push, &my_edges);
+        my_items += k;
         int32_t delta = push.pushed - k;
         if (lane == 0 && delta != 0) atomicAdd(work, delta);
         push.pushed = 0;
         // keep one iteration's worth (this warp's own continuation), share the rest
         if (push.count > 32) push.spill(32);
+    }
+    // work done by this warp, for the kernel ledger (items expanded, edges scanned)
+    for (int o = 16; o > 0; o >>= 1) my_edges += __shfl_down_sync(0xFFFFFFFFu, my_edges, o);
+    if (lane == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(a.ctr + CTR_ASYNC_ITEMS), (unsigned long long)my_items);
+        atomicAdd(reinterpret_cast<unsigned long long*>(a.ctr + CTR_ASYNC_EDGES), (unsigned long long)my_edges);
     }
 }
 
@@ -439,10 +537,21 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
             init[CTR_ATAIL - CTR_AHEAD] = qlen;
             init[CTR_AWORK - CTR_AHEAD] = qlen;
             SCC_CUDA(cudaMemcpyAsync(s->ctr + CTR_AHEAD, init, sizeof(init), cudaMemcpyHostToDevice, s->stream));
+            SCC_TRY(scc_zero_counters(s, CTR_ASYNC_ITEMS, 4));
+            if (s->ledger_on) SCC_CUDA(cudaEventRecord(s->lev[0], s->stream));
             k_reach_async<<<async_blocks(s->device), REACH_THREADS, 0, s->stream>>>(a, s->aq, qcap);
             SCC_LAUNCHED(s);
+            if (s->ledger_on) SCC_CUDA(cudaEventRecord(s->lev[1], s->stream));
             s->traversal_steps++;
             SCC_TRY(scc_sync_counters(s));
+            if (s->ledger_on) {
+                float ms = 0.f;
+                SCC_CUDA(cudaEventElapsedTime(&ms, s->lev[0], s->lev[1]));
+                s->ledger_ms += ms;
+                s->ledger_launches++;
+                s->ledger_items += *reinterpret_cast<long long*>(s->h_ctr + CTR_ASYNC_ITEMS);
+                s->ledger_edges += *reinterpret_cast<long long*>(s->h_ctr + CTR_ASYNC_EDGES);
+            }
             if (scc_trace_on()) {
                 double t1 = now_ms();
                 fprintf(stderr, "[scc] reach async seeds=%d spilled=%d %.3f ms\n", qlen, s->h_ctr[CTR_ATAIL], t1 - t0);

@@ -220,11 +220,14 @@ extern "C" int scc_state_free(scc_state* s) {
     if (!s) return SCC_OK;
     cudaSetDevice(s->device);
     cudaFree(s->color); cudaFree(s->scc); cudaFree(s->wcc); cudaFree(s->live); cudaFree(s->live_tmp);
-    cudaFree(s->qa); cudaFree(s->qb); cudaFree(s->aq); cudaFree(s->uf); cudaFree(s->hq); cudaFree(s->hoff); cudaFree(s->mark); cudaFree(s->aux); cudaFree(s->block_sums);
+    cudaFree(s->qa); cudaFree(s->qb); cudaFree(s->aq); cudaFree(s->uf); cudaFree(s->hq); cudaFree(s->hoff); cudaFree(s->cnt_out); cudaFree(s->cnt_in); cudaFree(s->mark); cudaFree(s->aux); cudaFree(s->block_sums);
     cudaFree(s->ctr);
     if (s->h_ctr) cudaFreeHost(s->h_ctr);
     cudaFree(s->slot_key); cudaFree(s->slot_pivot); cudaFree(s->slot_fw); cudaFree(s->slot_bw); cudaFree(s->slot_count);
-    if (s->events) for (int i = 0; i < 16; ++i) cudaEventDestroy(s->ev[i]);
+    if (s->events) {
+        for (int i = 0; i < 16; ++i) cudaEventDestroy(s->ev[i]);
+        for (int i = 0; i < 2; ++i) cudaEventDestroy(s->lev[i]);
+    }
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return SCC_OK;
@@ -251,6 +254,8 @@ extern "C" int scc_state_create(const scc_graph* g, scc_state** out) {
     if (e == cudaSuccess) e = cudaMalloc(&s->qb, qb);
     if (e == cudaSuccess) e = cudaMalloc(&s->aq, qb);
     if (e == cudaSuccess) e = cudaMalloc(&s->uf, nb);
+    if (e == cudaSuccess) e = cudaMalloc(&s->cnt_out, nb);
+    if (e == cudaSuccess) e = cudaMalloc(&s->cnt_in, nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->hq, qb);
     if (e == cudaSuccess) e = cudaMalloc(&s->hoff, sizeof(long long) * (size_t)(2 * n + 64));
     if (e == cudaSuccess) e = cudaMemset(s->aq, 0xFF, qb);
@@ -260,6 +265,7 @@ extern "C" int scc_state_create(const scc_graph* g, scc_state** out) {
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_ctr, sizeof(int32_t) * CTR_MAX);
     if (e == cudaSuccess) {
         for (int i = 0; i < 16 && e == cudaSuccess; ++i) e = cudaEventCreate(&s->ev[i]);
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaEventCreate(&s->lev[i]);
         s->events = (e == cudaSuccess);
     }
     if (e != cudaSuccess) {
@@ -271,6 +277,23 @@ extern "C" int scc_state_create(const scc_graph* g, scc_state** out) {
     if (st == SCC_OK) st = scc_state_reset(s);
     if (st != SCC_OK) { scc_state_free(s); return st; }
     *out = s;
+    return SCC_OK;
+}
+
+extern "C" int scc_state_profile(scc_state* s, int enable) {
+    SCC_REQUIRE(s, SCC_ERR_INVALID, "state is NULL");
+    s->ledger_on = enable != 0;
+    s->ledger_ms = 0.0;
+    s->ledger_launches = s->ledger_items = s->ledger_edges = 0;
+    return SCC_OK;
+}
+
+extern "C" int scc_state_profile_read(scc_state* s, double* ms, int64_t* launches, int64_t* items, int64_t* edges) {
+    SCC_REQUIRE(s, SCC_ERR_INVALID, "state is NULL");
+    if (ms) *ms = s->ledger_ms;
+    if (launches) *launches = s->ledger_launches;
+    if (items) *items = s->ledger_items;
+    if (edges) *edges = s->ledger_edges;
     return SCC_OK;
 }
 

@@ -154,6 +154,152 @@ __global__ void k_trim1_fresh(TrimArgs a, int32_t n) {
     block_count_add(a.ctr + CTR_COUNT, cnt);
 }
 
+// ------------------------------------------------------------------ counting peel
+// On a fresh state every vertex is live and of colour -1, so v's live
+// out-neighbour count is its out-degree minus its self-loops (a contiguous run
+// in the sorted list), from the offsets alone.  Peeling then needs one atomic
+// decrement per edge of a trimmed vertex: whoever brings a count to zero
+// trims that vertex (the colour CAS makes it happen once) and continues the
+// chain from it.  Counts track the live counts exactly, so the result is the
+// same fixpoint as the scanning peel.
+__device__ __forceinline__ int32_t self_run(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                                            int32_t v) {
+    int32_t b = __ldg(off + v), e = __ldg(off + v + 1);
+    if (b == e || __ldg(adj + b) > v || __ldg(adj + e - 1) < v) return 0;
+    int32_t lo = b, hi = e;                 // first entry >= v
+    while (lo < hi) { int32_t mid = (lo + hi) >> 1; if (__ldg(adj + mid) < v) lo = mid + 1; else hi = mid; }
+    int32_t first = lo;
+    hi = e;                                 // first entry > v
+    while (lo < hi) { int32_t mid = (lo + hi) >> 1; if (__ldg(adj + mid) <= v) lo = mid + 1; else hi = mid; }
+    return lo - first;
+}
+
+__global__ void k_count_init(const int32_t* __restrict__ begin, const int32_t* __restrict__ node_idx,
+                             const int32_t* __restrict__ r_begin, const int32_t* __restrict__ r_node_idx, int32_t n,
+                             int32_t* __restrict__ cnt_out, int32_t* __restrict__ cnt_in) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t v = (int32_t)i;
+        cnt_out[v] = (__ldg(begin + v + 1) - __ldg(begin + v)) - self_run(begin, node_idx, v);
+        cnt_in[v] = (__ldg(r_begin + v + 1) - __ldg(r_begin + v)) - self_run(r_begin, r_node_idx, v);
+    }
+}
+
+struct CountArgs {
+    const int32_t* begin; const int32_t* node_idx; const int32_t* r_begin; const int32_t* r_node_idx;
+    int32_t* color; int32_t* scc; int32_t* cnt_out; int32_t* cnt_in;
+    int32_t* ovf; int32_t* ctr;
+};
+
+__device__ __forceinline__ bool count_trim(const CountArgs& a, int32_t v) {
+    if (atomicCAS(a.color + v, SCC_COLOR_INIT, SCC_COLOR_DONE) != SCC_COLOR_INIT) return false;
+    a.scc[v] = v;
+    return true;
+}
+
+// Decrement the counts of x's neighbours; trimmed ones go on the stack.
+__device__ void count_cascade(const CountArgs& a, int32_t x0, int32_t& cnt) {
+    int32_t stk[TRIM_STACK];
+    int sp = 0;
+    stk[sp++] = x0;
+    while (sp > 0) {
+        int32_t x = stk[--sp];
+        int32_t ob = __ldg(a.begin + x), oe = __ldg(a.begin + x + 1);
+        int32_t ib = __ldg(a.r_begin + x), ie = __ldg(a.r_begin + x + 1);
+        if ((oe - ob) + (ie - ib) > TRIM_BIG_DEG) {
+            int32_t pos = atomicAdd(a.ctr + CTR_OVERFLOW, 1);
+            a.ovf[pos] = x;
+            continue;
+        }
+        // out-neighbour w loses an in-neighbour; in-neighbour u loses an out-neighbour
+        for (int32_t k = ob; k < oe; ++k) {
+            int32_t w = __ldg(a.node_idx + k);
+            if (w == x) continue;
+            if (atomicSub(a.cnt_in + w, 1) == 1 && count_trim(a, w)) {
+                cnt++;
+                if (sp < TRIM_STACK) stk[sp++] = w;
+                else { int32_t pos = atomicAdd(a.ctr + CTR_OVERFLOW, 1); a.ovf[pos] = w; }
+            }
+        }
+        for (int32_t k = ib; k < ie; ++k) {
+            int32_t u = __ldg(a.r_node_idx + k);
+            if (u == x) continue;
+            if (atomicSub(a.cnt_out + u, 1) == 1 && count_trim(a, u)) {
+                cnt++;
+                if (sp < TRIM_STACK) stk[sp++] = u;
+                else { int32_t pos = atomicAdd(a.ctr + CTR_OVERFLOW, 1); a.ovf[pos] = u; }
+            }
+        }
+    }
+}
+
+__global__ void k_count_peel(CountArgs a, int32_t n) {
+    int32_t cnt = 0;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t limit = (((int64_t)n + 31) / 32) * 32;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += stride) {
+        if (i < n) {
+            int32_t v = (int32_t)i;
+            if ((__ldcg(a.cnt_out + v) == 0 || __ldcg(a.cnt_in + v) == 0) && count_trim(a, v)) {
+                cnt++;
+                count_cascade(a, v, cnt);
+            }
+        }
+    }
+    block_count_add(a.ctr + CTR_COUNT, cnt);
+}
+
+// Overflow: one warp per trimmed high-degree (or deep-chain) vertex.
+__global__ void k_count_overflow(CountArgs a, const int32_t* __restrict__ items, int32_t n_items) {
+    int lane = threadIdx.x & 31;
+    int32_t cnt = 0;
+    int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t wi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; wi < n_items; wi += wstride) {
+        int32_t x = items[wi];
+        int32_t ob = __ldg(a.begin + x), oe = __ldg(a.begin + x + 1);
+        for (int32_t k = ob + lane; k < oe; k += 32) {
+            int32_t w = __ldg(a.node_idx + k);
+            if (w != x && atomicSub(a.cnt_in + w, 1) == 1 && count_trim(a, w)) { cnt++; count_cascade(a, w, cnt); }
+        }
+        int32_t ib = __ldg(a.r_begin + x), ie = __ldg(a.r_begin + x + 1);
+        for (int32_t k = ib + lane; k < ie; k += 32) {
+            int32_t u = __ldg(a.r_node_idx + k);
+            if (u != x && atomicSub(a.cnt_out + u, 1) == 1 && count_trim(a, u)) { cnt++; count_cascade(a, u, cnt); }
+        }
+    }
+    block_count_add(a.ctr + CTR_COUNT, cnt);
+}
+
+static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
+    int32_t n = g->n;
+    CountArgs a;
+    a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin; a.r_node_idx = g->r_node_idx;
+    a.color = s->color; a.scc = s->scc; a.cnt_out = s->cnt_out; a.cnt_in = s->cnt_in;
+    a.ovf = s->qa; a.ctr = s->ctr;
+    SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
+    SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
+    k_count_init<<<scc_blocks(n), SCC_THREADS, 0, s->stream>>>(g->begin, g->node_idx, g->r_begin, g->r_node_idx, n,
+                                                               s->cnt_out, s->cnt_in);
+    SCC_LAUNCHED(s);
+    k_count_peel<<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, n);
+    SCC_LAUNCHED(s);
+    int64_t total = 0;
+    for (int round = 0; round < 1000000; ++round) {
+        SCC_TRY(scc_sync_counters(s));
+        total += s->h_ctr[CTR_COUNT];
+        int32_t novf = s->h_ctr[CTR_OVERFLOW];
+        if (novf == 0) break;
+        SCC_CUDA(cudaMemcpyAsync(s->qb, s->qa, sizeof(int32_t) * (size_t)novf, cudaMemcpyDeviceToDevice, s->stream));
+        SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
+        SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
+        k_count_overflow<<<scc_blocks((int64_t)novf * 32, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, s->qb,
+                                                                                                          novf);
+        SCC_LAUNCHED(s);
+    }
+    *trimmed = (int32_t)total;
+    s->fresh = false;
+    return SCC_OK;
+}
+
 // Overflow expansion: one warp per already-trimmed vertex x, lanes stride its
 // neighbours; newly trimmed neighbours cascade per lane.
 __global__ void k_trim1_overflow(TrimArgs a, const int32_t* __restrict__ items, int32_t n_items,
@@ -213,6 +359,7 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
     if (n_items <= 0) return SCC_OK;
     // snapshot colours (aux) so overflowed vertices keep their pre-trim colour
     bool fresh = s->fresh && !use_live;
+    if (fresh && s->cnt_in) return trim1_counting(g, s, trimmed);
     if (fresh) {
         // every colour is -1: the snapshot the overflow path reads is that constant
         k_fill_aux<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(n_items, s->aux, SCC_COLOR_INIT);

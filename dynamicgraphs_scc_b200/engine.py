@@ -301,6 +301,31 @@ class State:
         call("scc_histogram", self.handle, i32p(sz), i32p(ct), k.value, C.byref(k))
         return dict(zip(sz.tolist(), ct.tolist()))
 
+    # -- updates (methods 5-11 of the reference) ------------------------------------------------
+    def update_batch(self, ins_src=(), ins_dst=(), del_src=(), del_dst=()) -> dict:
+        """Apply deletions then insertions to the graph and update the labels in place."""
+        a, b = _i32(ins_src), _i32(ins_dst)
+        c, d = _i32(del_src), _i32(del_dst)
+        if a.shape != b.shape or c.shape != d.shape:
+            raise ValueError("edge arrays differ in length")
+        st = capi.UpdateStats()
+        P = lambda x: x.ctypes.data_as(C.c_void_p) if x.size else None  # noqa: E731
+        call("scc_update_batch", self._g(), self.handle, int(a.size), P(a), P(b), int(c.size), P(c), P(d), 0,
+             C.byref(st))
+        return st.as_dict()
+
+    def incremental_insert(self, src, dst) -> dict:
+        return self.update_batch(ins_src=src, ins_dst=dst)
+
+    def decremental_delete(self, src, dst) -> dict:
+        return self.update_batch(del_src=src, del_dst=dst)
+
+    def insert_idea1(self, src, dst) -> dict:
+        s, d = _i32(src), _i32(dst)
+        st = capi.RunStats()
+        call("scc_insert_idea1", self._g(), self.handle, int(s.size), i32p(s), i32p(d), C.byref(st))
+        return st.as_dict()
+
     def free(self) -> None:
         if self._h is not None:
             capi.lib().scc_state_free(self._h)
@@ -311,6 +336,16 @@ class State:
             self.free()
         except Exception:
             pass
+
+
+def condensation_graph(graph: Graph, labels, num_sccs: int, ins_src=(), ins_dst=()) -> Graph:
+    """create_scc_edges + insert_idea2: the condensation over SCC ids plus inserted cross edges."""
+    lab = _i32(labels)
+    s, d = _i32(ins_src), _i32(ins_dst)
+    h = C.c_void_p()
+    call("scc_condensation_graph", graph.handle, i32p(lab), num_sccs, int(s.size), i32p(s) if s.size else None,
+         i32p(d) if d.size else None, C.byref(h))
+    return Graph(h)
 
 
 def read_scc_list(path: str, n: int):

@@ -123,6 +123,13 @@ int scc_state_get_wcc(scc_state* s, int32_t* wcc);
 /* Compact trim targets (get_compact_trim_targets, src/scc_trim1.cc:32). */
 int scc_state_get_trim_targets(scc_state* s, int32_t* out, int32_t capacity, int32_t* count);
 int scc_state_device_arrays(scc_state* s, int32_t** d_color, int32_t** d_scc);
+/* Kernel ledger (no counterpart in the reference; its phase timers are
+ * gettimeofday, src/scc_main.cc:180-184): when enabled, every launch of the
+ * asynchronous reachability drain is timed with CUDA events on the state's
+ * stream and its work counted (items expanded, edges scanned).  Enabling or
+ * disabling resets the totals. */
+int scc_state_profile(scc_state* s, int enable);
+int scc_state_profile_read(scc_state* s, double* ms, int64_t* launches, int64_t* items, int64_t* edges);
 
 /* ---- colour (src/scc_color.cc) --------------------------------------------------------- */
 int scc_get_new_color(scc_state* s, int32_t* color);          /* get_new_color,  scc_color.cc:38-54 */
@@ -251,6 +258,43 @@ int scc_output_scc_list(scc_state* s, const char* path);
 int scc_read_scc_list(const char* path, int32_t n, int32_t* labels, int32_t* num_sccs);
 /* create_histogram_and_print (scc_post_analyze.cc:235-261): sizes[i], counts[i] ascending by size. */
 int scc_histogram(scc_state* s, int32_t* sizes, int32_t* counts, int32_t capacity, int32_t* num_bins);
+
+/* ---- updates (src/scc_incremental.cc, src/scc_decremental.cc, src/common_main.h:180-393) -- */
+typedef struct scc_update_stats {
+    double ms_total, ms_merge, ms_delete, ms_insert;   /* device time: CSR merge, split, merge phases */
+    int32_t affected_delete;    /* vertices re-decomposed because their SCC lost an internal edge */
+    int32_t affected_insert;    /* vertices in the merge region FW(inserted targets) & BW(inserted sources) */
+    int64_t m_after;            /* edges after the batch */
+    int32_t num_sccs;           /* SCC count after the batch */
+} scc_update_stats;
+
+/* Apply a batch to a graph whose state holds a complete decomposition (after
+ * scc_run or a previous update): every copy of each deleted (u,v) is removed,
+ * each inserted (u,v) is added (add_edge semantics: duplicates kept), on the
+ * CSR and the transpose, lists kept sorted.  Labels are then recomputed only
+ * where they can change: SCCs that lost an internal edge (the decremental
+ * idea of delete_idea1 / method 9, src/scc_decremental.cc:7-24,
+ * src/scc_trim1.cc:61-66) and the region reachable from the targets and
+ * reaching the sources of inserted cross-SCC edges (where every merge of the
+ * condensation graph of methods 6/7/11 happens, src/common_main.h:180-314).
+ * on_device = 1: the four batch arrays are device pointers. */
+int scc_update_batch(scc_graph* g, scc_state* s, int64_t n_ins, const int32_t* ins_src, const int32_t* ins_dst,
+                     int64_t n_del, const int32_t* del_src, const int32_t* del_dst, int on_device,
+                     scc_update_stats* stats);
+int scc_incremental_insert(scc_graph* g, scc_state* s, int64_t n_ins, const int32_t* src, const int32_t* dst,
+                           scc_update_stats* stats);
+int scc_decremental_delete(scc_graph* g, scc_state* s, int64_t n_del, const int32_t* src, const int32_t* dst,
+                           scc_update_stats* stats);
+/* insert_idea1 (src/scc_incremental.cc:7-17, method 5): add the edges, then
+ * reset the state and decompose from scratch. */
+int scc_insert_idea1(scc_graph* g, scc_state* s, int64_t n_ins, const int32_t* src, const int32_t* dst,
+                     scc_run_stats* stats);
+/* create_scc_edges + insert_idea2 (src/common_main.h:180-314, src/scc_incremental.cc:19-27,
+ * methods 6/7/11): the condensation graph over SCC ids labels[v] in [0, num_sccs)
+ * (host array, e.g. from scc_read_scc_list), with every cross-SCC edge of g and of
+ * the inserted batch (host arrays) mapped to (id(u), id(v)), duplicates dropped. */
+int scc_condensation_graph(const scc_graph* g, const int32_t* labels, int32_t num_sccs, int64_t n_ins,
+                           const int32_t* ins_src, const int32_t* ins_dst, scc_graph** out);
 
 /* One-call convenience: host CSR in, canonical labels out (H2D + run + D2H). */
 int scc_decompose_csr(int32_t n, int32_t m, const int32_t* begin, const int32_t* node_idx,
