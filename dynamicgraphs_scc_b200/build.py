@@ -31,6 +31,8 @@ CU_SOURCES = [
     "scc_gen.cu",
     "scc_noalloc.cu",
     "scc_update.cu",
+    "scc_tune.cu",
+    "scc_server.cu",
 ]
 
 

@@ -56,11 +56,38 @@ class UpdateStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("session", C.c_int32), ("latency_ms", C.c_double), ("queue_ms", C.c_double),
+                ("update", UpdateStats)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_int64), ("rejected", C.c_int64), ("updates", C.c_int64),
+                ("max_inflight", C.c_int64), ("bytes_in_use", C.c_int64), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("max_ms", C.c_double), ("updates_per_s", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Tuning(C.Structure):
+    _fields_ = [(k, C.c_int32) for k in ("bu_alpha", "bu_div", "async_max", "async_after", "async_keep",
+                                         "async_blocks_per_sm", "huge_deg")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class GenParams(C.Structure):
     _fields_ = [
         ("rmat_scale", C.c_int), ("edge_factor", C.c_int), ("grid_side", C.c_int), ("num_cycles", C.c_int),
         ("cycle_min", C.c_int), ("cycle_max", C.c_int), ("seed", C.c_uint64),
     ]
+
+
+class BatchParams(C.Structure):
+    _fields_ = [("num_graphs", C.c_int32), ("n_min", C.c_int32), ("n_max", C.c_int32), ("mean_degree", C.c_double),
+                ("rmat_fraction", C.c_double), ("seed", C.c_uint64)]
 
 
 _P = C.c_void_p
@@ -99,6 +126,9 @@ _SIGS = {
     "scc_state_get_trim_targets": [_P, _I32P, C.c_int32, _I32P],
     "scc_state_device_arrays": [_P, C.POINTER(_P), C.POINTER(_P)],
     "scc_state_profile": [_P, C.c_int],
+    "scc_state_get_tuning": [_P, C.POINTER(Tuning)],
+    "scc_state_set_tuning": [_P, C.POINTER(Tuning)],
+    "scc_autotune": [_P, _P, C.c_int, C.c_int, C.POINTER(Tuning), C.POINTER(C.c_double)],
     "scc_state_profile_read": [_P, C.POINTER(C.c_double), _I64P, _I64P, _I64P],
     "scc_get_new_color": [_P, _I32P],
     "scc_get_curr_color": [_P, _I32P],
@@ -136,9 +166,22 @@ _SIGS = {
     "scc_decremental_delete": [_P, _P, C.c_int64, _I32P, _I32P, C.POINTER(UpdateStats)],
     "scc_insert_idea1": [_P, _P, C.c_int64, _I32P, _I32P, C.POINTER(RunStats)],
     "scc_condensation_graph": [_P, _I32P, C.c_int32, C.c_int64, _I32P, _I32P, C.POINTER(_P)],
+    "scc_server_create": [C.c_int, C.c_int, C.c_int64, C.POINTER(_P)],
+    "scc_server_add_graph": [_P, _P, _I32P],
+    "scc_server_submit": [_P, C.c_int32, C.c_int64, _I32P, _I32P, C.c_int64, _I32P, _I32P, _I64P],
+    "scc_server_wait": [_P, C.c_int64, C.POINTER(RequestResult)],
+    "scc_server_drain": [_P],
+    "scc_server_get_stats": [_P, C.POINTER(ServerStats)],
+    "scc_server_labels": [_P, C.c_int32, _I32P],
+    "scc_server_session_graph": [_P, C.c_int32, C.POINTER(_P)],
+    "scc_server_free": [_P],
     "scc_gen_sizes": [C.POINTER(GenParams), _I32P, _I64P],
     "scc_gen_edges_host": [C.POINTER(GenParams), _I32P, _I32P, C.c_int64, _I64P],
     "scc_gen_graph": [C.POINTER(GenParams), C.c_int, C.c_int, C.POINTER(_P)],
+    "scc_gen_batch_layout": [C.POINTER(BatchParams), _I32P, _I32P, _I64P],
+    "scc_gen_batch_edges_host": [C.POINTER(BatchParams), _I32P, _I32P, C.c_int64, _I64P],
+    "scc_gen_batch_graph": [C.POINTER(BatchParams), C.c_int, C.c_int, C.POINTER(_P)],
+    "scc_graph_subgraph": [_P, C.c_int32, C.c_int32, C.POINTER(_P)],
 }
 _RESTYPES = {"scc_status_string": C.c_char_p, "scc_last_error": C.c_char_p, "scc_version": C.c_int}
 

@@ -117,6 +117,8 @@ static RoundArgs round_args(const scc_graph* g, scc_state* s) {
     a.live = s->live; a.live_count = s->live_count;
     a.only_color = 0; a.use_only = 0;
     a.pivot_score = nullptr;
+    a.huge_deg = s->tune.huge_deg;
+    a.async_keep = s->tune.async_keep;
     return a;
 }
 

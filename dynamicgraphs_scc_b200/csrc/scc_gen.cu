@@ -180,3 +180,203 @@ extern "C" int scc_gen_graph(const scc_gen_params* p, int flags, int device, scc
     cudaFree(dst);
     return rc;
 }
+
+// ------------------------------------------------------------------ batched uneven graphs
+#include <cub/device/device_scan.cuh>
+
+struct BatchTables {
+    std::vector<int32_t> offsets;   // num_graphs + 1
+    uint32_t pois[SCC_POIS_K];
+    uint32_t rmat_thr;
+};
+
+static int batch_tables(const scc_batch_params* p, BatchTables& t) {
+    SCC_REQUIRE(p, SCC_ERR_INVALID, "params is NULL");
+    SCC_REQUIRE(p->num_graphs >= 1 && p->num_graphs <= (1 << 20), SCC_ERR_INVALID, "num_graphs %d", p->num_graphs);
+    SCC_REQUIRE(p->n_min >= 1 && p->n_max >= p->n_min && p->n_max <= (1 << 24), SCC_ERR_INVALID,
+                "vertex range [%d, %d]", p->n_min, p->n_max);
+    SCC_REQUIRE(p->mean_degree >= 0.0 && p->mean_degree <= 32.0, SCC_ERR_INVALID, "mean_degree %f", p->mean_degree);
+    SCC_REQUIRE(p->rmat_fraction >= 0.0 && p->rmat_fraction <= 1.0, SCC_ERR_INVALID, "rmat_fraction %f",
+                p->rmat_fraction);
+    t.offsets.assign((size_t)p->num_graphs + 1, 0);
+    double lo = log((double)p->n_min), hi = log((double)p->n_max);
+    int64_t total = 0;
+    for (int32_t g = 0; g < p->num_graphs; ++g) {
+        uint64_t r = scc_rand3(p->seed, 0xB47ull, (uint64_t)g);
+        double u = (double)(r >> 11) * (1.0 / 9007199254740992.0);
+        int64_t ni = (int64_t)floor(exp(lo + u * (hi - lo)));
+        if (ni < p->n_min) ni = p->n_min;
+        if (ni > p->n_max) ni = p->n_max;
+        total += ni;
+        SCC_REQUIRE(total < SCC_WCC_ROOT_MASK, SCC_ERR_INVALID, "batch too large (%lld vertices)", (long long)total);
+        t.offsets[(size_t)g + 1] = (int32_t)total;
+    }
+    // Poisson(mean) CDF thresholds
+    double pk = exp(-p->mean_degree), cdf = 0.0;
+    for (int k = 0; k < SCC_POIS_K; ++k) {
+        if (k > 0) pk *= p->mean_degree / k;
+        cdf += pk;
+        double x = cdf * 4294967296.0;
+        t.pois[k] = (k == SCC_POIS_K - 1 || x >= 4294967295.0) ? 0xFFFFFFFFu : (uint32_t)x;
+    }
+    double rt = p->rmat_fraction * 4294967296.0;
+    t.rmat_thr = rt >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)rt;
+    return SCC_OK;
+}
+
+extern "C" int scc_gen_batch_layout(const scc_batch_params* p, int32_t* offsets, int32_t* n, int64_t* max_edges) {
+    BatchTables t;
+    SCC_TRY(batch_tables(p, t));
+    if (offsets) memcpy(offsets, t.offsets.data(), sizeof(int32_t) * t.offsets.size());
+    if (n) *n = t.offsets.back();
+    if (max_edges) *max_edges = (int64_t)t.offsets.back() * SCC_BATCH_MAX_DEG;
+    return SCC_OK;
+}
+
+extern "C" int scc_gen_batch_edges_host(const scc_batch_params* p, int32_t* src, int32_t* dst, int64_t capacity,
+                                        int64_t* m) {
+    BatchTables t;
+    SCC_TRY(batch_tables(p, t));
+    SCC_REQUIRE(src && dst && m, SCC_ERR_INVALID, "NULL argument");
+    int64_t k = 0;
+    for (int32_t g = 0; g < p->num_graphs; ++g) {
+        uint64_t gs = scc_batch_graph_seed(p->seed, (uint32_t)g);
+        int32_t base = t.offsets[(size_t)g];
+        uint32_t ni = (uint32_t)(t.offsets[(size_t)g + 1] - base);
+        for (uint32_t lv = 0; lv < ni; ++lv) {
+            int d = scc_batch_degree(t.pois, gs, lv);
+            SCC_REQUIRE(k + d <= capacity, SCC_ERR_INVALID, "capacity %lld too small", (long long)capacity);
+            for (int j = 0; j < d; ++j) {
+                src[k] = base + (int32_t)lv;
+                dst[k] = base + (int32_t)scc_batch_target(gs, lv, (uint32_t)j, ni, t.rmat_thr);
+                k++;
+            }
+        }
+    }
+    *m = k;
+    return SCC_OK;
+}
+
+struct BatchDev {
+    const int32_t* offsets; int32_t num_graphs; uint64_t seed; uint32_t rmat_thr; uint32_t pois[SCC_POIS_K];
+};
+
+__device__ __forceinline__ int32_t batch_graph_of(const BatchDev& b, int32_t v) {
+    int32_t lo = 0, hi = b.num_graphs - 1;
+    while (lo < hi) { int32_t mid = (lo + hi + 1) >> 1; if (b.offsets[mid] <= v) lo = mid; else hi = mid - 1; }
+    return lo;
+}
+
+__global__ void k_batch_degree(BatchDev b, int32_t n, int64_t* __restrict__ deg) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t v = (int32_t)i, g = batch_graph_of(b, v);
+        deg[i] = scc_batch_degree(b.pois, scc_batch_graph_seed(b.seed, (uint32_t)g), (uint32_t)(v - b.offsets[g]));
+    }
+}
+
+__global__ void k_batch_edges(BatchDev b, int32_t n, const int64_t* __restrict__ eoff, int32_t* __restrict__ src,
+                              int32_t* __restrict__ dst) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t v = (int32_t)i, g = batch_graph_of(b, v);
+        int32_t base = b.offsets[g];
+        uint32_t ni = (uint32_t)(b.offsets[g + 1] - base), lv = (uint32_t)(v - base);
+        uint64_t gs = scc_batch_graph_seed(b.seed, (uint32_t)g);
+        int d = scc_batch_degree(b.pois, gs, lv);
+        int64_t o = eoff[i];
+        for (int j = 0; j < d; ++j) {
+            src[o + j] = v;
+            dst[o + j] = base + (int32_t)scc_batch_target(gs, lv, (uint32_t)j, ni, b.rmat_thr);
+        }
+    }
+}
+
+extern "C" int scc_gen_batch_graph(const scc_batch_params* p, int flags, int device, scc_graph** out) {
+    BatchTables t;
+    SCC_TRY(batch_tables(p, t));
+    SCC_REQUIRE(out, SCC_ERR_INVALID, "out is NULL");
+    SCC_CUDA(cudaSetDevice(device));
+    int32_t n = t.offsets.back();
+    int32_t* d_off = nullptr;
+    int64_t *deg = nullptr, *eoff = nullptr;
+    SCC_CUDA(cudaMalloc(&d_off, sizeof(int32_t) * t.offsets.size()));
+    SCC_CUDA(cudaMalloc(&deg, sizeof(int64_t) * ((size_t)n + 1)));
+    SCC_CUDA(cudaMalloc(&eoff, sizeof(int64_t) * ((size_t)n + 1)));
+    SCC_CUDA(cudaMemcpy(d_off, t.offsets.data(), sizeof(int32_t) * t.offsets.size(), cudaMemcpyHostToDevice));
+    SCC_CUDA(cudaMemset(deg, 0, sizeof(int64_t) * ((size_t)n + 1)));
+    BatchDev b;
+    b.offsets = d_off; b.num_graphs = p->num_graphs; b.seed = p->seed; b.rmat_thr = t.rmat_thr;
+    memcpy(b.pois, t.pois, sizeof(t.pois));
+    k_batch_degree<<<scc_blocks(n, 256, 148 * 64), 256>>>(b, n, deg);
+    SCC_CUDA(cudaPeekAtLastError());
+    size_t bytes = 0;
+    void* tmp = nullptr;
+    SCC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, deg, eoff, n + 1));
+    SCC_CUDA(cudaMalloc(&tmp, bytes > 0 ? bytes : 16));
+    SCC_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, deg, eoff, n + 1));
+    int64_t m = 0;
+    SCC_CUDA(cudaMemcpy(&m, eoff + n, sizeof(int64_t), cudaMemcpyDeviceToHost));
+    cudaFree(tmp);
+    int32_t *src = nullptr, *dst = nullptr;
+    SCC_CUDA(cudaMalloc(&src, sizeof(int32_t) * (size_t)(m > 0 ? m : 1)));
+    SCC_CUDA(cudaMalloc(&dst, sizeof(int32_t) * (size_t)(m > 0 ? m : 1)));
+    k_batch_edges<<<scc_blocks(n, 256, 148 * 64), 256>>>(b, n, eoff, src, dst);
+    SCC_CUDA(cudaPeekAtLastError());
+    SCC_CUDA(cudaDeviceSynchronize());
+    cudaFree(deg); cudaFree(eoff); cudaFree(d_off);
+    int rc = scc_impl_build_graph_from_device_edges(n, m, src, dst, flags, device, out);
+    cudaFree(src); cudaFree(dst);
+    return rc;
+}
+
+// ------------------------------------------------------------------ subgraph of a closed id range
+__global__ void k_sub_offsets(const int32_t* __restrict__ off, int32_t vb, int32_t nv, int32_t* __restrict__ out) {
+    int32_t base = off[vb];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= nv; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = off[vb + i] - base;
+}
+
+__global__ void k_sub_adj(const int32_t* __restrict__ adj, int64_t e0, int64_t cnt, int32_t vb, int32_t nv,
+                          int32_t* __restrict__ out, int* __restrict__ bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t w = adj[e0 + i] - vb;
+        if (w < 0 || w >= nv) { atomicExch(bad, 1); w = 0; }
+        out[i] = w;
+    }
+}
+
+extern "C" int scc_graph_subgraph(const scc_graph* g, int32_t v_begin, int32_t v_end, scc_graph** out) {
+    SCC_REQUIRE(g && out, SCC_ERR_INVALID, "NULL argument");
+    SCC_REQUIRE(v_begin >= 0 && v_end >= v_begin && v_end <= g->n, SCC_ERR_INVALID, "range [%d, %d)", v_begin, v_end);
+    SCC_CUDA(cudaSetDevice(g->device));
+    int32_t nv = v_end - v_begin;
+    int32_t h[4];
+    SCC_CUDA(cudaMemcpy(&h[0], g->begin + v_begin, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    SCC_CUDA(cudaMemcpy(&h[1], g->begin + v_end, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    SCC_CUDA(cudaMemcpy(&h[2], g->r_begin + v_begin, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    SCC_CUDA(cudaMemcpy(&h[3], g->r_begin + v_end, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    int64_t m = h[1] - h[0];
+    SCC_REQUIRE(h[3] - h[2] == m, SCC_ERR_INVALID, "range [%d, %d) has edges leaving it", v_begin, v_end);
+    scc_graph* s = new scc_graph();
+    s->device = g->device; s->n = nv; s->m = m;
+    int* bad = nullptr;
+    cudaError_t e = cudaMalloc(&s->begin, sizeof(int32_t) * ((size_t)nv + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->r_begin, sizeof(int32_t) * ((size_t)nv + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->node_idx, sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->r_node_idx, sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+    if (e == cudaSuccess) e = cudaMalloc(&bad, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(bad, 0, sizeof(int));
+    if (e != cudaSuccess) { scc_graph_free(s); cudaFree(bad); return scc_cuda_status(e, "subgraph", __FILE__, __LINE__); }
+    k_sub_offsets<<<scc_blocks(nv + 1), 256>>>(g->begin, v_begin, nv, s->begin);
+    k_sub_offsets<<<scc_blocks(nv + 1), 256>>>(g->r_begin, v_begin, nv, s->r_begin);
+    if (m > 0) {
+        k_sub_adj<<<scc_blocks(m), 256>>>(g->node_idx, h[0], m, v_begin, nv, s->node_idx, bad);
+        k_sub_adj<<<scc_blocks(m), 256>>>(g->r_node_idx, h[2], m, v_begin, nv, s->r_node_idx, bad);
+    }
+    int hb = 0;
+    e = cudaMemcpy(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(bad);
+    if (e != cudaSuccess) { scc_graph_free(s); return scc_cuda_status(e, "subgraph", __FILE__, __LINE__); }
+    if (hb) { scc_graph_free(s); scc_set_error("range [%d, %d) has edges leaving it", v_begin, v_end); return SCC_ERR_INVALID; }
+    *out = s;
+    return SCC_OK;
+}

@@ -105,6 +105,44 @@ SCC_HD int scc_grid_edges(uint64_t seed, uint32_t side, uint32_t base, uint64_t 
     return 1;
 }
 
+// ---- batched uneven graphs
+// Poisson CDF in 32-bit fixed point, thr[k] = floor(P(X <= k) * 2^32), built on
+// the host; a draw is the first k with u < thr[k].
+#define SCC_POIS_K 64
+#define SCC_BATCH_MAX_DEG 255
+SCC_HD int scc_poisson_draw(const uint32_t* thr, uint32_t u) {
+    int k = 0;
+    while (k < SCC_POIS_K - 1 && u >= thr[k]) ++k;
+    return k < SCC_BATCH_MAX_DEG ? k : SCC_BATCH_MAX_DEG;
+}
+
+SCC_HD uint64_t scc_batch_graph_seed(uint64_t seed, uint32_t g) {
+    return scc_mix64(seed ^ (0xBA7C4ull + (uint64_t)g * 0x9E3779B97F4A7C15ull));
+}
+
+SCC_HD int scc_ceil_log2(uint32_t n) {
+    int s = 0;
+    while ((1ull << s) < (uint64_t)n) ++s;
+    return s;
+}
+
+SCC_HD int scc_batch_degree(const uint32_t* thr, uint64_t gseed, uint32_t lv) {
+    return scc_poisson_draw(thr, (uint32_t)(scc_rand3(gseed, lv, 0) >> 32));
+}
+
+// Target of edge j of local vertex lv in a graph of n vertices: R-MAT column
+// (reduced mod n) with probability rmat_thr / 2^32, else uniform.
+SCC_HD uint32_t scc_batch_target(uint64_t gseed, uint32_t lv, uint32_t j, uint32_t n, uint32_t rmat_thr) {
+    uint64_t r = scc_rand3(gseed, lv, 1 + (uint64_t)j);
+    if ((uint32_t)r < rmat_thr) {
+        uint32_t s, d;
+        int scale = scc_ceil_log2(n);
+        scc_rmat_edge(gseed ^ 0x77ull, scale > 0 ? scale : 1, ((uint64_t)lv << 8) | j, &s, &d);
+        return d % n;
+    }
+    return (uint32_t)(((r >> 32) * (uint64_t)n) >> 32);
+}
+
 // Vertex of position `i` on planted cycle `k` (distinct within a cycle for
 // i < 2^bits, since scc_scramble is a bijection).
 SCC_HD uint32_t scc_cycle_vertex(uint64_t seed, uint32_t k, uint32_t i, int bits) {

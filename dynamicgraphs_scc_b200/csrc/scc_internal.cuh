@@ -39,6 +39,7 @@ struct scc_graph {
     int32_t* r_begin = nullptr;   // [n+1]  in-CSR offsets       (gm_graph::r_begin)
     int32_t* r_node_idx = nullptr;// [m]    in-neighbours        (gm_graph::r_node_idx)
     bool owns = true;
+    bool async_arrays = false;    // arrays come from cudaMallocAsync (after an update)
 };
 
 // Device counters block (one allocation, mirrored to pinned host memory).
@@ -121,6 +122,10 @@ struct scc_state {
 
     cudaEvent_t ev[16];
     bool events = false;
+
+    // defaults from a B200 sweep on the mixed R-MAT + grid workload (fewer
+    // resident warps in the drain mean less contention on its queue)
+    scc_tuning tune = {14, 24, 1 << 14, 1, 16, 1, 4096};
 
     // kernel ledger (scc_state_profile): device time and algorithmic bytes of
     // the asynchronous reachability drain, timed with events on `stream`

@@ -26,19 +26,15 @@
 #include <stdlib.h>
 #include "scc_round.cuh"
 
-#define BU_DIV 24               // bottom-up when frontier > 2*live/BU_DIV
-#define ASYNC_MAX (1 << 16)     // narrow frontier
-#define ASYNC_AFTER 2           // consecutive narrow levels before draining asynchronously
+// switch points come from the state's tunables (scc_tuning)
 #define ASYNC_EMPTY (-1)
 #define ASYNC_IDLE_LIMIT (1 << 22)
 #define ASYNC_SLOT_LIMIT (1 << 20)
-#define ASYNC_SPILL_KEEP 64
 
 // ------------------------------------------------------------------ warp expansion
 // Expand one item per lane (valid lanes only); push(p, item) is warp-collective.
-// Items whose degree exceeds HUGE_DEG are handed to k_reach_huge (edge-parallel
+// Items whose degree exceeds a.huge_deg are handed to k_reach_huge (edge-parallel
 // over the whole grid) when huge_list is given, so one hub never serialises a level.
-#define HUGE_DEG 4096
 template <class Push>
 __device__ __forceinline__ void expand_warp(const RoundArgs& a, bool valid, int32_t it, Push& push,
                                             int32_t* huge_list = nullptr, int32_t* huge_cnt = nullptr,
@@ -53,7 +49,7 @@ __device__ __forceinline__ void expand_warp(const RoundArgs& a, bool valid, int3
         e = __ldg(off + v + 1);
         c = __ldg(a.color + v);
         if (edge_acc) *edge_acc += e - b;
-        if (huge_list && e - b > HUGE_DEG) {
+        if (huge_list && e - b > a.huge_deg) {
             huge_list[atomicAdd(huge_cnt, 1)] = it;
             e = b;
         }
@@ -284,6 +280,7 @@ struct LocalPush {
     int32_t count;         // warp-uniform
     int32_t pushed;        // items added since the last work-counter update
     int32_t* q; int32_t* tail; int32_t* work; int64_t qcap; int32_t* err;
+    int32_t keep;          // items kept for this warp when sharing
     __device__ __forceinline__ void spill(int32_t keep) {
         int lane = threadIdx.x & 31;
         __syncwarp();
@@ -314,7 +311,7 @@ struct LocalPush {
         int32_t k = __popc(bal);
         count += k;
         pushed += k;
-        if (count > WBUF - 32) spill(ASYNC_SPILL_KEEP);
+        if (count > WBUF - 32) spill(keep > 64 ? keep : 64);
     }
 };
 
@@ -405,7 +402,7 @@ __global__ void __launch_bounds__(REACH_THREADS) k_reach_async(RoundArgs a, int3
     int32_t* tail = a.ctr + CTR_ATAIL;
     int32_t* work = a.ctr + CTR_AWORK;
     int32_t* err = a.ctr + CTR_ERROR;
-    LocalPush push{sbuf[wid], sbeg[wid], send[wid], 0, 0, q, tail, work, qcap, err};
+    LocalPush push{sbuf[wid], sbeg[wid], send[wid], 0, 0, q, tail, work, qcap, err, a.async_keep};
     int idle = 0;
     int32_t last_work = -1;
     long long my_edges = 0;     // per lane
@@ -469,7 +466,7 @@ __global__ void __launch_bounds__(REACH_THREADS) k_reach_async(RoundArgs a, int3
         if (lane == 0 && delta != 0) atomicAdd(work, delta);
         push.pushed = 0;
         // keep one iteration's worth (this warp's own continuation), share the rest
-        if (push.count > 32) push.spill(32);
+        if (push.count > push.keep) push.spill(push.keep);
     }
     // work done by this warp, for the kernel ledger (items expanded, edges scanned)
     for (int o = 16; o > 0; o >>= 1) my_edges += __shfl_down_sync(0xFFFFFFFFu, my_edges, o);
@@ -486,19 +483,24 @@ bool scc_trace_on() {
     return t == 1;
 }
 
-static int async_blocks(int device) {
-    static int cached[64] = {0};
-    if (device >= 0 && device < 64 && cached[device]) return cached[device];
+static int async_blocks(int device, int want_per_sm) {
+    static int cached_sms[64] = {0}, cached_per[64] = {0};
     int sms = 148, per = 1;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_reach_async, REACH_THREADS, 0);
+    if (device >= 0 && device < 64 && cached_sms[device]) {
+        sms = cached_sms[device];
+        per = cached_per[device];
+    } else {
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_reach_async, REACH_THREADS, 0);
+        if (per < 1) per = 1;
+        if (device >= 0 && device < 64) { cached_sms[device] = sms; cached_per[device] = per; }
+    }
+    // every block must be resident (warps wait on each other's items): never
+    // more than the occupancy limit; a few per SM cover a narrow frontier
+    // without flooding the queue with pollers
+    if (want_per_sm < per) per = want_per_sm;
     if (per < 1) per = 1;
-    // every block must be resident (warps wait on each other's items); two per SM
-    // (16 warps) cover a narrow frontier without flooding the queue with pollers
-    if (per > 2) per = 2;
-    int b = sms * per;
-    if (device >= 0 && device < 64) cached[device] = b;
-    return b;
+    return sms * per;
 }
 
 static double now_ms() {
@@ -509,9 +511,8 @@ static double now_ms() {
 
 // Direction choice (Beamer's rule as in the reference's BFS state machine,
 // gm_bfs_template.h:418-487): go bottom-up when the next frontier's edges
-// times BU_ALPHA exceed the edges of the vertices being traversed; stay
-// bottom-up while the frontier holds more than 2*live/BU_DIV items.
-#define BU_ALPHA 14
+// times bu_alpha exceed the edges of the vertices being traversed; stay
+// bottom-up while the frontier holds more than 2*live/bu_div items.
 
 int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen) {
     int32_t* qin = s->qa;
@@ -530,7 +531,7 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
             SCC_LAUNCHED(s);
             narrow = 0;
             mode = "bottom-up";
-        } else if (qlen <= ASYNC_MAX && narrow >= ASYNC_AFTER) {
+        } else if (qlen <= s->tune.async_max && narrow >= s->tune.async_after) {
             int64_t qcap = 2LL * s->n + 64;
             SCC_CUDA(cudaMemcpyAsync(s->aq, qin, sizeof(int32_t) * (size_t)qlen, cudaMemcpyDeviceToDevice, s->stream));
             int32_t init[CTR_AWORK - CTR_AHEAD + 1] = {0};   // head, tail, work on separate lines
@@ -539,7 +540,7 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
             SCC_CUDA(cudaMemcpyAsync(s->ctr + CTR_AHEAD, init, sizeof(init), cudaMemcpyHostToDevice, s->stream));
             SCC_TRY(scc_zero_counters(s, CTR_ASYNC_ITEMS, 4));
             if (s->ledger_on) SCC_CUDA(cudaEventRecord(s->lev[0], s->stream));
-            k_reach_async<<<async_blocks(s->device), REACH_THREADS, 0, s->stream>>>(a, s->aq, qcap);
+            k_reach_async<<<async_blocks(s->device, s->tune.async_blocks_per_sm), REACH_THREADS, 0, s->stream>>>(a, s->aq, qcap);
             SCC_LAUNCHED(s);
             if (s->ledger_on) SCC_CUDA(cudaEventRecord(s->lev[1], s->stream));
             s->traversal_steps++;
@@ -583,17 +584,17 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
         SCC_TRY(scc_sync_counters(s));
         int32_t next = s->h_ctr[CTR_QLEN];
         if (bottom_up) {
-            bottom_up = (int64_t)next * BU_DIV > live2;
+            bottom_up = (int64_t)next * s->tune.bu_div > live2;
         } else {
             unsigned long long fe = *reinterpret_cast<unsigned long long*>(s->h_ctr + CTR_EDGES);
-            bottom_up = fe * BU_ALPHA > live_edges;
+            bottom_up = fe * (unsigned long long)s->tune.bu_alpha > live_edges;
         }
         if (scc_trace_on()) {
             double t1 = now_ms();
             fprintf(stderr, "[scc] reach %s in=%d out=%d %.3f ms\n", mode, qlen, next, t1 - t0);
             t0 = t1;
         }
-        narrow = (!bottom_up && next <= ASYNC_MAX) ? narrow + 1 : 0;
+        narrow = (!bottom_up && next <= s->tune.async_max) ? narrow + 1 : 0;
         qlen = next;
         int32_t* t = qin; qin = qout; qout = t;
     }

@@ -17,6 +17,8 @@ struct RoundArgs {
     int32_t only_color;   // used when use_only
     int32_t use_only;
     const float* pivot_score;   // optional learned score per vertex (nullptr = degree rule)
+    int32_t huge_deg;           // top-down items above this degree go edge-parallel
+    int32_t async_keep;         // items a warp keeps before sharing in the asynchronous drain
 };
 
 __device__ __forceinline__ uint32_t pivot_hash(uint32_t v) {

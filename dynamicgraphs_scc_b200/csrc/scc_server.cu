@@ -1,0 +1,282 @@
+// Serving loop for streaming edge updates (the streaming configuration; the
+// reference has no server: its dynamic methods 5-11 read one insert or delete
+// file per process, src/common_main.h:500-732).
+//
+// Sessions are device-resident graphs with their decomposition (graph + state,
+// each state on its own CUDA stream).  Clients submit edge batches; worker
+// threads ("slots") run scc_update_batch.  Continuous batching: a request is
+// admitted as soon as a slot is free, its session has no request running (a
+// session's requests run in arrival order) and its device-memory estimate fits
+// the HBM budget next to everything resident and in flight; requests of
+// different sessions therefore overlap on the device.  A request that could
+// never fit the budget is rejected with SCC_ERR_OOM.  Latency = completion -
+// submission (host clock); p50/p99 and updates/s are kept.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <string.h>
+#include "scc_internal.cuh"
+
+struct ServerRequest {
+    int64_t id = 0;
+    int32_t session = 0;
+    std::vector<int32_t> ins_src, ins_dst, del_src, del_dst;
+    int64_t est_bytes = 0;
+    double t_submit = 0, t_start = 0, t_done = 0;
+    int rc = SCC_OK;
+    scc_update_stats st;
+    bool done = false;
+};
+
+struct ServerSession {
+    scc_graph* g = nullptr;
+    scc_state* s = nullptr;
+    bool busy = false;
+    int64_t resident = 0;
+};
+
+struct scc_server {
+    int device = 0;
+    int64_t budget = 0;
+    int64_t in_use = 0;          // resident sessions + admitted requests
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::vector<ServerSession> sessions;
+    std::unordered_map<int64_t, std::unique_ptr<ServerRequest>> reqs;
+    std::deque<int64_t> queue;
+    std::vector<std::thread> workers;
+    bool stop = false;
+    int64_t next_id = 1;
+    std::vector<double> latencies;
+    int64_t updates_done = 0, completed = 0, rejected = 0, max_inflight = 0, inflight = 0;
+    double t_first = -1.0, t_last = 0.0;
+};
+
+static double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+static int64_t graph_bytes(int32_t n, int64_t m) { return 8LL * ((int64_t)n + 1) + 8LL * m; }
+// state: per-vertex arrays, queues and per-colour slots (scc_state_create)
+static int64_t state_bytes(int32_t n) { return 140LL * (int64_t)n + 4096; }
+// an update: new CSR + transpose, deleted flags, sorted keys, temporaries
+static int64_t update_bytes(int32_t n, int64_t m, int64_t k_ins, int64_t k_del) {
+    return 10LL * (m + k_ins) + 64LL * (k_ins + k_del) + 16LL * (int64_t)n + (1 << 20);
+}
+
+static void worker_main(scc_server* sv) {
+    cudaSetDevice(sv->device);
+    for (;;) {
+        ServerRequest* r = nullptr;
+        ServerSession* ses = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(sv->mu);
+            for (;;) {
+                if (sv->stop) return;
+                bool rejected_one = false;
+                std::vector<char> blocked(sv->sessions.size(), 0);
+                for (auto it = sv->queue.begin(); it != sv->queue.end(); ++it) {
+                    ServerRequest* c = sv->reqs[*it].get();
+                    ServerSession& s = sv->sessions[(size_t)c->session];
+                    if (blocked[(size_t)c->session] || s.busy) { blocked[(size_t)c->session] = 1; continue; }
+                    if (sv->in_use + c->est_bytes > sv->budget) {
+                        if (sv->inflight == 0) {   // can never fit: reject
+                            c->rc = SCC_ERR_OOM;
+                            c->done = true;
+                            c->t_done = now_ms();
+                            sv->rejected++;
+                            sv->completed++;
+                            sv->queue.erase(it);
+                            sv->cv_done.notify_all();
+                            rejected_one = true;
+                            break;
+                        }
+                        blocked[(size_t)c->session] = 1;
+                        continue;
+                    }
+                    r = c;
+                    ses = &s;
+                    sv->queue.erase(it);
+                    break;
+                }
+                if (r) break;
+                if (rejected_one) continue;   // the queue changed: scan again
+                sv->cv_work.wait(lk);
+            }
+            ses->busy = true;
+            sv->in_use += r->est_bytes;
+            sv->inflight++;
+            sv->max_inflight = std::max(sv->max_inflight, sv->inflight);
+            r->t_start = now_ms();
+        }
+        int rc = scc_update_batch(ses->g, ses->s, (int64_t)r->ins_src.size(), r->ins_src.data(), r->ins_dst.data(),
+                                  (int64_t)r->del_src.size(), r->del_src.data(), r->del_dst.data(), 0, &r->st);
+        {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            r->rc = rc;
+            r->t_done = now_ms();
+            r->done = true;
+            ses->busy = false;
+            sv->in_use -= r->est_bytes;
+            sv->in_use -= ses->resident;
+            ses->resident = graph_bytes(ses->g->n, ses->g->m) + state_bytes(ses->g->n);
+            sv->in_use += ses->resident;
+            sv->inflight--;
+            sv->completed++;
+            if (rc == SCC_OK) {
+                sv->latencies.push_back(r->t_done - r->t_submit);
+                sv->updates_done += (int64_t)(r->ins_src.size() + r->del_src.size());
+            }
+            sv->t_last = std::max(sv->t_last, r->t_done);
+            r->ins_src.clear(); r->ins_src.shrink_to_fit(); r->ins_dst.clear(); r->ins_dst.shrink_to_fit();
+            r->del_src.clear(); r->del_src.shrink_to_fit(); r->del_dst.clear(); r->del_dst.shrink_to_fit();
+        }
+        sv->cv_done.notify_all();
+        sv->cv_work.notify_all();
+    }
+}
+
+extern "C" int scc_server_create(int device, int num_slots, int64_t hbm_budget_bytes, scc_server** out) {
+    SCC_REQUIRE(out && num_slots >= 1 && num_slots <= 64 && hbm_budget_bytes > 0, SCC_ERR_INVALID, "bad argument");
+    SCC_CUDA(cudaSetDevice(device));
+    scc_server* sv = new scc_server();
+    sv->device = device;
+    sv->budget = hbm_budget_bytes;
+    for (int i = 0; i < num_slots; ++i) sv->workers.emplace_back(worker_main, sv);
+    *out = sv;
+    return SCC_OK;
+}
+
+// Takes ownership of g; decomposes it (method 2) before the session serves.
+extern "C" int scc_server_add_graph(scc_server* sv, scc_graph* g, int32_t* session) {
+    SCC_REQUIRE(sv && g && session, SCC_ERR_INVALID, "NULL argument");
+    int64_t need = graph_bytes(g->n, g->m) + state_bytes(g->n);
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        SCC_REQUIRE(sv->in_use + need <= sv->budget, SCC_ERR_OOM, "graph needs %lld bytes, budget left %lld",
+                    (long long)need, (long long)(sv->budget - sv->in_use));
+        sv->in_use += need;
+    }
+    scc_state* s = nullptr;
+    int rc = scc_state_create(g, &s);
+    scc_run_stats st;
+    if (rc == SCC_OK) rc = scc_run(g, s, SCC_METHOD_GLOBAL_WCC_FB, SCC_PIVOT_DEGREE, &st);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (rc != SCC_OK) {
+        sv->in_use -= need;
+        scc_state_free(s);
+        return rc;
+    }
+    ServerSession ses;
+    ses.g = g; ses.s = s; ses.resident = need;
+    sv->sessions.push_back(ses);
+    *session = (int32_t)sv->sessions.size() - 1;
+    return SCC_OK;
+}
+
+extern "C" int scc_server_submit(scc_server* sv, int32_t session, int64_t n_ins, const int32_t* ins_src,
+                                 const int32_t* ins_dst, int64_t n_del, const int32_t* del_src, const int32_t* del_dst,
+                                 int64_t* request_id) {
+    SCC_REQUIRE(sv && request_id, SCC_ERR_INVALID, "NULL argument");
+    SCC_REQUIRE(n_ins >= 0 && n_del >= 0 && (n_ins == 0 || (ins_src && ins_dst)) && (n_del == 0 || (del_src && del_dst)),
+                SCC_ERR_INVALID, "bad batch");
+    auto r = std::make_unique<ServerRequest>();
+    r->ins_src.assign(ins_src, ins_src + n_ins); r->ins_dst.assign(ins_dst, ins_dst + n_ins);
+    r->del_src.assign(del_src, del_src + n_del); r->del_dst.assign(del_dst, del_dst + n_del);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    SCC_REQUIRE(session >= 0 && session < (int32_t)sv->sessions.size(), SCC_ERR_INVALID, "no session %d", session);
+    const ServerSession& s = sv->sessions[(size_t)session];
+    r->session = session;
+    r->id = sv->next_id++;
+    r->est_bytes = update_bytes(s.g->n, s.g->m, n_ins, n_del);
+    r->t_submit = now_ms();
+    if (sv->t_first < 0) sv->t_first = r->t_submit;
+    *request_id = r->id;
+    sv->queue.push_back(r->id);
+    sv->reqs[r->id] = std::move(r);
+    sv->cv_work.notify_one();
+    return SCC_OK;
+}
+
+extern "C" int scc_server_wait(scc_server* sv, int64_t request_id, scc_request_result* out) {
+    SCC_REQUIRE(sv, SCC_ERR_INVALID, "NULL argument");
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->reqs.find(request_id);
+    SCC_REQUIRE(it != sv->reqs.end(), SCC_ERR_INVALID, "no request %lld", (long long)request_id);
+    ServerRequest* r = it->second.get();
+    sv->cv_done.wait(lk, [&] { return r->done; });
+    if (out) {
+        out->status = r->rc;
+        out->session = r->session;
+        out->latency_ms = r->t_done - r->t_submit;
+        out->queue_ms = (r->t_start > 0 ? r->t_start : r->t_done) - r->t_submit;
+        out->update = r->st;
+    }
+    return SCC_OK;
+}
+
+extern "C" int scc_server_drain(scc_server* sv) {
+    SCC_REQUIRE(sv, SCC_ERR_INVALID, "NULL argument");
+    std::unique_lock<std::mutex> lk(sv->mu);
+    sv->cv_done.wait(lk, [&] { return sv->queue.empty() && sv->inflight == 0; });
+    return SCC_OK;
+}
+
+extern "C" int scc_server_get_stats(scc_server* sv, scc_server_stats* out) {
+    SCC_REQUIRE(sv && out, SCC_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    memset(out, 0, sizeof(*out));
+    std::vector<double> l = sv->latencies;
+    std::sort(l.begin(), l.end());
+    auto pct = [&](double p) { return l.empty() ? 0.0 : l[(size_t)std::min<double>(l.size() - 1, p * (l.size() - 1) + 0.5)]; };
+    out->completed = sv->completed;
+    out->rejected = sv->rejected;
+    out->p50_ms = pct(0.50);
+    out->p99_ms = pct(0.99);
+    out->max_ms = l.empty() ? 0.0 : l.back();
+    out->updates = sv->updates_done;
+    double span = sv->t_last - sv->t_first;
+    out->updates_per_s = span > 0 ? sv->updates_done / (span * 1e-3) : 0.0;
+    out->max_inflight = sv->max_inflight;
+    out->bytes_in_use = sv->in_use;
+    return SCC_OK;
+}
+
+extern "C" int scc_server_labels(scc_server* sv, int32_t session, int32_t* labels) {
+    SCC_REQUIRE(sv && labels, SCC_ERR_INVALID, "NULL argument");
+    ServerSession* s = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        SCC_REQUIRE(session >= 0 && session < (int32_t)sv->sessions.size(), SCC_ERR_INVALID, "no session %d", session);
+        s = &sv->sessions[(size_t)session];
+        SCC_REQUIRE(!s->busy, SCC_ERR_STATE, "session %d is busy", session);
+    }
+    return scc_canonical_labels(s->s, labels);
+}
+
+extern "C" int scc_server_session_graph(scc_server* sv, int32_t session, scc_graph** g) {
+    SCC_REQUIRE(sv && g, SCC_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    SCC_REQUIRE(session >= 0 && session < (int32_t)sv->sessions.size(), SCC_ERR_INVALID, "no session %d", session);
+    *g = sv->sessions[(size_t)session].g;
+    return SCC_OK;
+}
+
+extern "C" int scc_server_free(scc_server* sv) {
+    if (!sv) return SCC_OK;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stop = true;
+    }
+    sv->cv_work.notify_all();
+    for (auto& t : sv->workers) t.join();
+    for (auto& s : sv->sessions) { scc_state_free(s.s); scc_graph_free(s.g); }
+    delete sv;
+    return SCC_OK;
+}

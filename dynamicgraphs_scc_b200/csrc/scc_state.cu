@@ -280,6 +280,26 @@ extern "C" int scc_state_create(const scc_graph* g, scc_state** out) {
     return SCC_OK;
 }
 
+extern "C" int scc_state_get_tuning(scc_state* s, scc_tuning* t) {
+    SCC_REQUIRE(s && t, SCC_ERR_INVALID, "NULL argument");
+    *t = s->tune;
+    return SCC_OK;
+}
+
+extern "C" int scc_state_set_tuning(scc_state* s, const scc_tuning* t) {
+    SCC_REQUIRE(s && t, SCC_ERR_INVALID, "NULL argument");
+    SCC_REQUIRE(t->async_keep <= 192, SCC_ERR_INVALID, "async_keep %d above 192", t->async_keep);
+    SCC_REQUIRE(t->async_blocks_per_sm <= 8, SCC_ERR_INVALID, "async_blocks_per_sm %d above 8", t->async_blocks_per_sm);
+    if (t->bu_alpha > 0) s->tune.bu_alpha = t->bu_alpha;
+    if (t->bu_div > 0) s->tune.bu_div = t->bu_div;
+    if (t->async_max > 0) s->tune.async_max = t->async_max;
+    if (t->async_after > 0) s->tune.async_after = t->async_after;
+    if (t->async_keep > 0) s->tune.async_keep = t->async_keep;
+    if (t->async_blocks_per_sm > 0) s->tune.async_blocks_per_sm = t->async_blocks_per_sm;
+    if (t->huge_deg > 0) s->tune.huge_deg = t->huge_deg;
+    return SCC_OK;
+}
+
 extern "C" int scc_state_profile(scc_state* s, int enable) {
     SCC_REQUIRE(s, SCC_ERR_INVALID, "state is NULL");
     s->ledger_on = enable != 0;

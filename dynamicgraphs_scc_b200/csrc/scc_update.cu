@@ -74,7 +74,8 @@ __global__ void k_upd_degrees(int32_t n, const int32_t* __restrict__ off, const 
 __global__ void k_upd_merge(int32_t n, const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                             const uint8_t* __restrict__ dead, const int32_t* __restrict__ ndead,
                             const unsigned long long* __restrict__ ins, const int32_t* __restrict__ ins_begin,
-                            const int32_t* __restrict__ new_off, int32_t* __restrict__ new_adj) {
+                            const int32_t* __restrict__ new_off, int32_t* __restrict__ new_adj,
+                            int32_t* __restrict__ kp) {
     int lane = threadIdx.x & 31;
     int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < n; w += wstride) {
@@ -86,16 +87,34 @@ __global__ void k_upd_merge(int32_t n, const int32_t* __restrict__ off, const in
             for (int32_t k = lane; k < e - b; k += 32) new_adj[nb + k] = adj[b + k];
             continue;
         }
-        if (lane == 0) {                              // changed list: two-pointer merge
-            int32_t i = b, j = 0, o = nb;
-            const unsigned long long* iv = ins + ins_begin[v];
-            while (i < e || j < nins) {
-                if (i < e && dead[i]) { ++i; continue; }
-                int32_t x = (i < e) ? adj[i] : INT32_MAX;
-                int32_t y = (j < nins) ? (int32_t)(uint32_t)iv[j] : INT32_MAX;
-                if (j >= nins || (i < e && x <= y)) { new_adj[o++] = x; ++i; }
-                else { new_adj[o++] = y; ++j; }
+        // Changed list, merged by the whole warp.  A kept old entry x lands at
+        // (kept entries before it) + (inserted entries < x); an inserted y at
+        // (its index) + (kept old entries <= y), so equal values keep old-first
+        // order.  kp[i] records the kept count before old position i.
+        const unsigned long long* iv = ins + ins_begin[v];
+        int32_t kept_base = 0;
+        for (int32_t i0 = b; i0 < e; i0 += 32) {
+            int32_t i = i0 + lane;
+            bool valid = i < e;
+            int32_t x = valid ? adj[i] : 0;
+            bool kept = valid && !dead[i];
+            unsigned bal = __ballot_sync(0xFFFFFFFFu, kept);
+            int32_t r = __popc(bal & ((1u << lane) - 1u));
+            if (valid) kp[i] = kept_base + r;
+            if (kept) {
+                int32_t lo = 0, hi = nins;
+                while (lo < hi) { int32_t mid = (lo + hi) >> 1; if ((int32_t)(uint32_t)iv[mid] < x) lo = mid + 1; else hi = mid; }
+                new_adj[nb + kept_base + r + lo] = x;
             }
+            kept_base += __popc(bal);
+        }
+        __syncwarp();
+        for (int32_t j = lane; j < nins; j += 32) {
+            int32_t y = (int32_t)(uint32_t)iv[j];
+            int32_t lo = b, hi = e;          // first old entry > y
+            while (lo < hi) { int32_t mid = (lo + hi) >> 1; if (adj[mid] <= y) lo = mid + 1; else hi = mid; }
+            int32_t before = (lo < e) ? kp[lo] : kept_base;
+            new_adj[nb + j + before] = y;
         }
         __syncwarp();
     }
@@ -170,30 +189,44 @@ __global__ void k_upd_colour_region(int32_t n, uint8_t* __restrict__ mark, int32
 }
 
 // ------------------------------------------------------------------ host helpers
+// Stream-ordered scratch: cudaFree would synchronise the whole device and
+// serialise updates that run concurrently on other streams.
 struct DevBuf {
     void* p = nullptr;
-    ~DevBuf() { if (p) cudaFree(p); }
+    cudaStream_t st = nullptr;
+    ~DevBuf() { if (p) cudaFreeAsync(p, st); }
     template <class T> T* as() { return (T*)p; }
 };
 
-static int alloc(DevBuf& b, size_t bytes) {
-    SCC_CUDA(cudaMalloc(&b.p, bytes > 0 ? bytes : 16));
+static int alloc(DevBuf& b, size_t bytes, cudaStream_t st) {
+    b.st = st;
+    SCC_CUDA(cudaMallocAsync(&b.p, bytes > 0 ? bytes : 16, st));
     return SCC_OK;
+}
+
+// Replace a graph's arrays with stream-ordered ones.
+static void release_graph_arrays(scc_graph* g, cudaStream_t st) {
+    int32_t* arr[4] = {g->begin, g->node_idx, g->r_begin, g->r_node_idx};
+    for (int i = 0; i < 4; ++i) {
+        if (!arr[i]) continue;
+        if (g->async_arrays) cudaFreeAsync(arr[i], st);
+        else cudaFree(arr[i]);
+    }
 }
 
 // keys (a<<32|b) sorted ascending into out (k entries); invalid ids flagged in *bad.
 static int sorted_keys(int64_t k, const int32_t* d_a, const int32_t* d_b, int32_t n, cudaStream_t st,
                        DevBuf& out, int* d_bad) {
     DevBuf tmpk, tmp;
-    SCC_TRY(alloc(out, sizeof(unsigned long long) * (size_t)k));
-    SCC_TRY(alloc(tmpk, sizeof(unsigned long long) * (size_t)k));
+    SCC_TRY(alloc(out, sizeof(unsigned long long) * (size_t)k, st));
+    SCC_TRY(alloc(tmpk, sizeof(unsigned long long) * (size_t)k, st));
     if (k == 0) return SCC_OK;
     k_upd_keys<<<scc_blocks(k), SCC_THREADS, 0, st>>>(k, d_a, d_b, n, tmpk.as<unsigned long long>(), d_bad);
     SCC_CUDA(cudaPeekAtLastError());
     size_t bytes = 0;
     SCC_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, bytes, tmpk.as<unsigned long long>(), out.as<unsigned long long>(),
                                             (int)k, 0, 64, st));
-    SCC_TRY(alloc(tmp, bytes));
+    SCC_TRY(alloc(tmp, bytes, st));
     SCC_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, bytes, tmpk.as<unsigned long long>(), out.as<unsigned long long>(),
                                             (int)k, 0, 64, st));
     return SCC_OK;
@@ -203,11 +236,12 @@ static int sorted_keys(int64_t k, const int32_t* d_a, const int32_t* d_b, int32_
 static int merge_side(int32_t n, int64_t m, const int32_t* off, const int32_t* adj, const unsigned long long* del,
                       int64_t kdel, const unsigned long long* ins, int64_t kins, cudaStream_t st, int32_t** new_off,
                       int32_t** new_adj, int64_t* new_m) {
-    DevBuf dead, ndead, insb, deg, tmp;
-    SCC_TRY(alloc(dead, (size_t)(m > 0 ? m : 1)));
-    SCC_TRY(alloc(ndead, sizeof(int32_t) * (size_t)n));
-    SCC_TRY(alloc(insb, sizeof(int32_t) * (size_t)n));
-    SCC_TRY(alloc(deg, sizeof(int32_t) * ((size_t)n + 1)));
+    DevBuf dead, ndead, insb, deg, tmp, kp;
+    SCC_TRY(alloc(kp, sizeof(int32_t) * (size_t)(m > 0 ? m : 1), st));
+    SCC_TRY(alloc(dead, (size_t)(m > 0 ? m : 1), st));
+    SCC_TRY(alloc(ndead, sizeof(int32_t) * (size_t)n, st));
+    SCC_TRY(alloc(insb, sizeof(int32_t) * (size_t)n, st));
+    SCC_TRY(alloc(deg, sizeof(int32_t) * ((size_t)n + 1), st));
     SCC_CUDA(cudaMemsetAsync(dead.p, 0, (size_t)(m > 0 ? m : 1), st));
     SCC_CUDA(cudaMemsetAsync(ndead.p, 0, sizeof(int32_t) * (size_t)n, st));
     SCC_CUDA(cudaMemsetAsync(deg.p, 0, sizeof(int32_t) * ((size_t)n + 1), st));
@@ -222,20 +256,21 @@ static int merge_side(int32_t n, int64_t m, const int32_t* off, const int32_t* a
         SCC_CUDA(cudaPeekAtLastError());
     }
     int32_t* noff = nullptr;
-    SCC_CUDA(cudaMalloc(&noff, sizeof(int32_t) * ((size_t)n + 1)));
+    SCC_CUDA(cudaMallocAsync(&noff, sizeof(int32_t) * ((size_t)n + 1), st));
     size_t bytes = 0;
     SCC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, deg.as<int32_t>(), noff, n + 1, st));
-    SCC_TRY(alloc(tmp, bytes));
+    SCC_TRY(alloc(tmp, bytes, st));
     SCC_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, bytes, deg.as<int32_t>(), noff, n + 1, st));
     int32_t nm = 0;
     SCC_CUDA(cudaMemcpyAsync(&nm, noff + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     SCC_CUDA(cudaStreamSynchronize(st));
     int32_t* nadj = nullptr;
-    cudaError_t e = cudaMalloc(&nadj, sizeof(int32_t) * (size_t)(nm > 0 ? nm : 1));
-    if (e != cudaSuccess) { cudaFree(noff); return scc_cuda_status(e, "cudaMalloc", __FILE__, __LINE__); }
+    cudaError_t e = cudaMallocAsync(&nadj, sizeof(int32_t) * (size_t)(nm > 0 ? nm : 1), st);
+    if (e != cudaSuccess) { cudaFreeAsync(noff, st); return scc_cuda_status(e, "cudaMallocAsync", __FILE__, __LINE__); }
     if (n > 0) {
         k_upd_merge<<<scc_blocks((int64_t)n * 32, SCC_THREADS, 148 * 16), SCC_THREADS, 0, st>>>(
-            n, off, adj, dead.as<uint8_t>(), ndead.as<int32_t>(), ins, insb.as<int32_t>(), noff, nadj);
+            n, off, adj, dead.as<uint8_t>(), ndead.as<int32_t>(), ins, insb.as<int32_t>(), noff, nadj,
+            kp.as<int32_t>());
         SCC_CUDA(cudaPeekAtLastError());
     }
     SCC_CUDA(cudaStreamSynchronize(st));
@@ -253,6 +288,8 @@ static RoundArgs update_round_args(const scc_graph* g, scc_state* s) {
     a.live = s->live; a.live_count = s->live_count;
     a.only_color = 0; a.use_only = 1;
     a.pivot_score = nullptr;
+    a.huge_deg = s->tune.huge_deg;
+    a.async_keep = s->tune.async_keep;
     return a;
 }
 
@@ -282,8 +319,8 @@ extern "C" int scc_update_batch(scc_graph* g, scc_state* s, int64_t n_ins, const
     DevBuf d_is, d_id, d_ds, d_dd, bad;
     const int32_t *is = ins_src, *id = ins_dst, *ds = del_src, *dd = del_dst;
     if (!on_device) {
-        SCC_TRY(alloc(d_is, sizeof(int32_t) * (size_t)n_ins)); SCC_TRY(alloc(d_id, sizeof(int32_t) * (size_t)n_ins));
-        SCC_TRY(alloc(d_ds, sizeof(int32_t) * (size_t)n_del)); SCC_TRY(alloc(d_dd, sizeof(int32_t) * (size_t)n_del));
+        SCC_TRY(alloc(d_is, sizeof(int32_t) * (size_t)n_ins, st)); SCC_TRY(alloc(d_id, sizeof(int32_t) * (size_t)n_ins, st));
+        SCC_TRY(alloc(d_ds, sizeof(int32_t) * (size_t)n_del, st)); SCC_TRY(alloc(d_dd, sizeof(int32_t) * (size_t)n_del, st));
         if (n_ins) {
             SCC_CUDA(cudaMemcpyAsync(d_is.p, ins_src, sizeof(int32_t) * (size_t)n_ins, cudaMemcpyHostToDevice, st));
             SCC_CUDA(cudaMemcpyAsync(d_id.p, ins_dst, sizeof(int32_t) * (size_t)n_ins, cudaMemcpyHostToDevice, st));
@@ -294,7 +331,7 @@ extern "C" int scc_update_batch(scc_graph* g, scc_state* s, int64_t n_ins, const
         }
         is = d_is.as<int32_t>(); id = d_id.as<int32_t>(); ds = d_ds.as<int32_t>(); dd = d_dd.as<int32_t>();
     }
-    SCC_TRY(alloc(bad, sizeof(int)));
+    SCC_TRY(alloc(bad, sizeof(int), st));
     SCC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
     DevBuf ins_k, ins_t, del_k, del_t;
     SCC_TRY(sorted_keys(n_ins, is, id, n, st, ins_k, bad.as<int>()));
@@ -313,9 +350,10 @@ extern "C" int scc_update_batch(scc_graph* g, scc_state* s, int64_t n_ins, const
                        ins_k.as<unsigned long long>(), n_ins, st, &nb, &na, &m1));
     int rc = merge_side(n, g->m, g->r_begin, g->r_node_idx, del_t.as<unsigned long long>(), n_del,
                         ins_t.as<unsigned long long>(), n_ins, st, &nrb, &nra, &m2);
-    if (rc != SCC_OK) { cudaFree(nb); cudaFree(na); return rc; }
-    cudaFree(g->begin); cudaFree(g->node_idx); cudaFree(g->r_begin); cudaFree(g->r_node_idx);
+    if (rc != SCC_OK) { cudaFreeAsync(nb, st); cudaFreeAsync(na, st); return rc; }
+    release_graph_arrays(g, st);
     g->begin = nb; g->node_idx = na; g->r_begin = nrb; g->r_node_idx = nra; g->m = m1;
+    g->async_arrays = true;
     SCC_CUDA(cudaEventRecord(s->ev[9], st));
 
     // 2. deletions: re-decompose the SCCs that lost an internal edge
@@ -404,12 +442,12 @@ extern "C" int scc_insert_idea1(scc_graph* g, scc_state* s, int64_t n_ins, const
     SCC_CUDA(cudaSetDevice(s->device));
     cudaStream_t st = s->stream;
     DevBuf d_s, d_d, bad, ins_k, ins_t;
-    SCC_TRY(alloc(d_s, sizeof(int32_t) * (size_t)n_ins)); SCC_TRY(alloc(d_d, sizeof(int32_t) * (size_t)n_ins));
+    SCC_TRY(alloc(d_s, sizeof(int32_t) * (size_t)n_ins, st)); SCC_TRY(alloc(d_d, sizeof(int32_t) * (size_t)n_ins, st));
     if (n_ins) {
         SCC_CUDA(cudaMemcpyAsync(d_s.p, src, sizeof(int32_t) * (size_t)n_ins, cudaMemcpyHostToDevice, st));
         SCC_CUDA(cudaMemcpyAsync(d_d.p, dst, sizeof(int32_t) * (size_t)n_ins, cudaMemcpyHostToDevice, st));
     }
-    SCC_TRY(alloc(bad, sizeof(int)));
+    SCC_TRY(alloc(bad, sizeof(int), st));
     SCC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
     SCC_TRY(sorted_keys(n_ins, d_s.as<int32_t>(), d_d.as<int32_t>(), g->n, st, ins_k, bad.as<int>()));
     SCC_TRY(sorted_keys(n_ins, d_d.as<int32_t>(), d_s.as<int32_t>(), g->n, st, ins_t, bad.as<int>()));
@@ -421,8 +459,9 @@ extern "C" int scc_insert_idea1(scc_graph* g, scc_state* s, int64_t n_ins, const
                        &na, &m1));
     SCC_TRY(merge_side(g->n, g->m, g->r_begin, g->r_node_idx, nullptr, 0, ins_t.as<unsigned long long>(), n_ins, st,
                        &nrb, &nra, &m2));
-    cudaFree(g->begin); cudaFree(g->node_idx); cudaFree(g->r_begin); cudaFree(g->r_node_idx);
+    release_graph_arrays(g, st);
     g->begin = nb; g->node_idx = na; g->r_begin = nrb; g->r_node_idx = nra; g->m = m1;
+    g->async_arrays = true;
     SCC_TRY(scc_state_reset(s));
     return scc_run(g, s, SCC_METHOD_GLOBAL_WCC_FB, SCC_PIVOT_DEGREE, stats);
 }
@@ -466,13 +505,14 @@ extern "C" int scc_condensation_graph(const scc_graph* g, const int32_t* labels,
     cudaStream_t st;
     SCC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     int64_t total = g->m + n_ins;
-    DevBuf lab, src, dst, bs, bd, bad;
     int rc = SCC_OK;
-    if ((rc = alloc(lab, sizeof(int32_t) * (size_t)g->n)) == SCC_OK &&
-        (rc = alloc(src, sizeof(int32_t) * (size_t)total)) == SCC_OK &&
-        (rc = alloc(dst, sizeof(int32_t) * (size_t)total)) == SCC_OK &&
-        (rc = alloc(bs, sizeof(int32_t) * (size_t)n_ins)) == SCC_OK &&
-        (rc = alloc(bd, sizeof(int32_t) * (size_t)n_ins)) == SCC_OK && (rc = alloc(bad, sizeof(int))) == SCC_OK) {
+    {   // buffers are freed on `st` before it is destroyed
+    DevBuf lab, src, dst, bs, bd, bad;
+    if ((rc = alloc(lab, sizeof(int32_t) * (size_t)g->n, st)) == SCC_OK &&
+        (rc = alloc(src, sizeof(int32_t) * (size_t)total, st)) == SCC_OK &&
+        (rc = alloc(dst, sizeof(int32_t) * (size_t)total, st)) == SCC_OK &&
+        (rc = alloc(bs, sizeof(int32_t) * (size_t)n_ins, st)) == SCC_OK &&
+        (rc = alloc(bd, sizeof(int32_t) * (size_t)n_ins, st)) == SCC_OK && (rc = alloc(bad, sizeof(int), st)) == SCC_OK) {
         cudaMemsetAsync(bad.p, 0, sizeof(int), st);
         cudaMemcpyAsync(lab.p, labels, sizeof(int32_t) * (size_t)g->n, cudaMemcpyHostToDevice, st);
         if (g->n > 0)
@@ -495,6 +535,8 @@ extern "C" int scc_condensation_graph(const scc_graph* g, const int32_t* labels,
         else rc = scc_impl_build_graph_from_device_edges(num_sccs, total, src.as<int32_t>(), dst.as<int32_t>(),
                                                           SCC_BUILD_DEDUP | SCC_BUILD_NO_SELF_LOOPS, g->device, out);
     }
+    }
+    cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
     return rc;
 }

@@ -72,6 +72,23 @@ class Graph:
         call("scc_gen_graph", C.byref(p), flags, device, C.byref(h))
         return cls(h)
 
+    @classmethod
+    def generate_batch(cls, num_graphs=4096, n_min=1024, n_max=65536, mean_degree=6.0, rmat_fraction=0.3, seed=1,
+                       flags=capi.SCC_BUILD_DEDUP | capi.SCC_BUILD_NO_SELF_LOOPS, device=0):
+        """Disjoint union of many seeded uneven graphs; returns (graph, per-graph vertex offsets)."""
+        p = capi.BatchParams(num_graphs, n_min, n_max, mean_degree, rmat_fraction, seed)
+        offs = np.empty(num_graphs + 1, np.int32)
+        call("scc_gen_batch_layout", C.byref(p), i32p(offs), None, None)
+        h = C.c_void_p()
+        call("scc_gen_batch_graph", C.byref(p), flags, device, C.byref(h))
+        return cls(h), offs
+
+    def subgraph(self, v_begin: int, v_end: int) -> "Graph":
+        """Induced subgraph on a closed id range (one graph of a batch), rebased to 0."""
+        h = C.c_void_p()
+        call("scc_graph_subgraph", self.handle, v_begin, v_end, C.byref(h))
+        return Graph(h)
+
     # -- properties ---------------------------------------------------------------------------
     @property
     def handle(self) -> C.c_void_p:
@@ -125,6 +142,18 @@ def generate_edges_host(**kw):
     m = C.c_int64()
     call("scc_gen_edges_host", C.byref(p), i32p(src), i32p(dst), cap.value, C.byref(m))
     return n.value, src[:m.value], dst[:m.value]
+
+
+def generate_batch_edges_host(num_graphs=8, n_min=1024, n_max=65536, mean_degree=6.0, rmat_fraction=0.3, seed=1):
+    """Raw edges of a seeded batch on the host: (n, offsets, src, dst)."""
+    p = capi.BatchParams(num_graphs, n_min, n_max, mean_degree, rmat_fraction, seed)
+    offs = np.empty(num_graphs + 1, np.int32)
+    n = C.c_int32(); cap = C.c_int64()
+    call("scc_gen_batch_layout", C.byref(p), i32p(offs), C.byref(n), C.byref(cap))
+    src = np.empty(max(cap.value, 1), np.int32); dst = np.empty(max(cap.value, 1), np.int32)
+    m = C.c_int64()
+    call("scc_gen_batch_edges_host", C.byref(p), i32p(src), i32p(dst), cap.value, C.byref(m))
+    return n.value, offs, src[:m.value], dst[:m.value]
 
 
 class State:
@@ -188,6 +217,27 @@ class State:
 
     def synchronize(self) -> None:
         call("scc_state_synchronize", self.handle)
+
+    def get_tuning(self) -> dict:
+        t = capi.Tuning()
+        call("scc_state_get_tuning", self.handle, C.byref(t))
+        return t.as_dict()
+
+    def autotune(self, method: int = METHOD_GLOBAL_WCC_FB, max_trials: int = 32):
+        """Grid-search the tunables on this state's graph; keeps and returns the fastest."""
+        t = capi.Tuning()
+        ms = C.c_double()
+        call("scc_autotune", self._g(), self.handle, method, max_trials, C.byref(t), C.byref(ms))
+        return t.as_dict(), ms.value
+
+    def set_tuning(self, **kw) -> None:
+        """Change traversal tunables (keys of scc_tuning); unspecified keys keep their value."""
+        t = capi.Tuning(*([0] * 7))
+        for k, v in kw.items():
+            if not hasattr(t, k):
+                raise KeyError(k)
+            setattr(t, k, int(v))
+        call("scc_state_set_tuning", self.handle, C.byref(t))
 
     # -- colour ----------------------------------------------------------------------------------
     def get_new_color(self) -> int:
@@ -329,6 +379,73 @@ class State:
     def free(self) -> None:
         if self._h is not None:
             capi.lib().scc_state_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Server:
+    """Serving loop: device-resident graphs updated by streamed edge batches
+    (continuous batching over worker slots, HBM-budget admission)."""
+
+    def __init__(self, num_slots: int = 4, hbm_budget_bytes: int = 64 << 30, device: int = 0):
+        h = C.c_void_p()
+        call("scc_server_create", device, num_slots, hbm_budget_bytes, C.byref(h))
+        self._h = h
+        self.sizes = {}
+
+    def add_graph(self, graph: Graph) -> int:
+        """Takes ownership of the graph (the Python object is emptied) and decomposes it."""
+        sid = C.c_int32()
+        n = graph.num_nodes()
+        call("scc_server_add_graph", self._h, graph.handle, C.byref(sid))
+        graph._h = None
+        self.sizes[sid.value] = n
+        return sid.value
+
+    def submit(self, session: int, ins_src=(), ins_dst=(), del_src=(), del_dst=()) -> int:
+        a, b, c, d = _i32(ins_src), _i32(ins_dst), _i32(del_src), _i32(del_dst)
+        rid = C.c_int64()
+        call("scc_server_submit", self._h, session, int(a.size), i32p(a), i32p(b), int(c.size), i32p(c), i32p(d),
+             C.byref(rid))
+        return rid.value
+
+    def wait(self, request_id: int) -> dict:
+        r = capi.RequestResult()
+        call("scc_server_wait", self._h, request_id, C.byref(r))
+        out = {"status": r.status, "session": r.session, "latency_ms": r.latency_ms, "queue_ms": r.queue_ms}
+        out.update(r.update.as_dict())
+        return out
+
+    def drain(self) -> None:
+        call("scc_server_drain", self._h)
+
+    def stats(self) -> dict:
+        s = capi.ServerStats()
+        call("scc_server_get_stats", self._h, C.byref(s))
+        return s.as_dict()
+
+    def labels(self, session: int) -> np.ndarray:
+        a = np.empty(self.sizes[session], np.int32)
+        call("scc_server_labels", self._h, session, i32p(a))
+        return a
+
+    def session_csr(self, session: int):
+        h = C.c_void_p()
+        call("scc_server_session_graph", self._h, session, C.byref(h))
+        g = Graph(h)
+        try:
+            return g.csr()
+        finally:
+            g._h = None       # borrowed
+
+    def free(self) -> None:
+        if self._h is not None:
+            capi.lib().scc_server_free(self._h)
             self._h = None
 
     def __del__(self):

@@ -131,6 +131,25 @@ int scc_state_device_arrays(scc_state* s, int32_t** d_color, int32_t** d_scc);
 int scc_state_profile(scc_state* s, int enable);
 int scc_state_profile_read(scc_state* s, double* ms, int64_t* launches, int64_t* items, int64_t* edges);
 
+/* Traversal tunables (the reference hard-codes its BFS switch points,
+ * gm_graph/inc/gm_bfs_template.h:418-487, 841-842): the autotuner
+ * (scc_autotune) and callers may change them per state.  Any value <= 0
+ * keeps the current setting. */
+typedef struct scc_tuning {
+    int32_t bu_alpha;             /* bottom-up when frontier edges * bu_alpha > traversed edges (14) */
+    int32_t bu_div;               /* stay bottom-up while frontier > 2 * live / bu_div (24) */
+    int32_t async_max;            /* a frontier this small counts as narrow (16384) */
+    int32_t async_after;          /* narrow levels before the asynchronous drain (1) */
+    int32_t async_keep;           /* items a warp keeps for itself before sharing (16, max 192) */
+    int32_t async_blocks_per_sm;  /* resident blocks per SM in the drain (1, max 8) */
+    int32_t huge_deg;             /* degree above which a top-down item is expanded edge-parallel (4096) */
+} scc_tuning;
+int scc_state_get_tuning(scc_state* s, scc_tuning* t);
+int scc_state_set_tuning(scc_state* s, const scc_tuning* t);
+/* Autotuner: times up to max_trials full decompositions (method) of g under
+ * candidate tunings, keeps the fastest in s, resets s, and reports it. */
+int scc_autotune(const scc_graph* g, scc_state* s, int method, int max_trials, scc_tuning* best, double* best_ms);
+
 /* ---- colour (src/scc_color.cc) --------------------------------------------------------- */
 int scc_get_new_color(scc_state* s, int32_t* color);          /* get_new_color,  scc_color.cc:38-54 */
 int scc_get_curr_color(scc_state* s, int32_t* color);         /* get_curr_color, scc_color.cc:56-61 */
@@ -295,6 +314,39 @@ int scc_insert_idea1(scc_graph* g, scc_state* s, int64_t n_ins, const int32_t* s
  * the inserted batch (host arrays) mapped to (id(u), id(v)), duplicates dropped. */
 int scc_condensation_graph(const scc_graph* g, const int32_t* labels, int32_t num_sccs, int64_t n_ins,
                            const int32_t* ins_src, const int32_t* ins_dst, scc_graph** out);
+
+/* ---- serving loop (no counterpart in the reference, whose dynamic methods read one
+ * update file per process, src/common_main.h:500-732) ----------------------------------- */
+typedef struct scc_server scc_server;
+typedef struct scc_request_result {
+    int status;                 /* SCC_OK, or SCC_ERR_OOM when the batch can never fit the budget */
+    int32_t session;
+    double latency_ms;          /* completion - submission */
+    double queue_ms;            /* admission - submission */
+    scc_update_stats update;
+} scc_request_result;
+typedef struct scc_server_stats {
+    int64_t completed, rejected, updates, max_inflight, bytes_in_use;
+    double p50_ms, p99_ms, max_ms, updates_per_s;
+} scc_server_stats;
+
+/* num_slots worker threads; admission keeps resident graphs + admitted batches
+ * under hbm_budget_bytes (estimates).  Requests of different sessions overlap
+ * on the device (one stream per session); a session's requests run in order. */
+int scc_server_create(int device, int num_slots, int64_t hbm_budget_bytes, scc_server** out);
+/* Takes ownership of g and decomposes it (method 2); *session names it. */
+int scc_server_add_graph(scc_server* sv, scc_graph* g, int32_t* session);
+/* Copies the batch (host arrays) and queues it; returns at once. */
+int scc_server_submit(scc_server* sv, int32_t session, int64_t n_ins, const int32_t* ins_src, const int32_t* ins_dst,
+                      int64_t n_del, const int32_t* del_src, const int32_t* del_dst, int64_t* request_id);
+int scc_server_wait(scc_server* sv, int64_t request_id, scc_request_result* out);
+int scc_server_drain(scc_server* sv);
+int scc_server_get_stats(scc_server* sv, scc_server_stats* out);
+/* Canonical labels of an idle session (n ints). */
+int scc_server_labels(scc_server* sv, int32_t session, int32_t* labels);
+/* The session's graph (owned by the server; valid until scc_server_free). */
+int scc_server_session_graph(scc_server* sv, int32_t session, scc_graph** g);
+int scc_server_free(scc_server* sv);
 
 /* One-call convenience: host CSR in, canonical labels out (H2D + run + D2H). */
 int scc_decompose_csr(int32_t n, int32_t m, const int32_t* begin, const int32_t* node_idx,

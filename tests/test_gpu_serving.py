@@ -1,0 +1,94 @@
+"""GPU: the serving loop.  Each session's results must be the same when its
+requests run alone and when they run mixed with other sessions' requests on
+several slots (continuous batching), and equal to the oracle; admission
+rejects what can never fit the HBM budget."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from dynamicgraphs_scc_b200 import Graph, Server
+from tests.test_gpu_update import apply_batch
+from tests.helpers import random_graph, seeded_graph
+
+pytestmark = pytest.mark.gpu
+
+
+def sessions_and_batches():
+    graphs = []
+    for seed in (1, 2):
+        n, s, d, _ = seeded_graph(rmat_scale=12, edge_factor=6, seed=seed)
+        graphs.append((n, s, d))
+    n, s, d, _ = seeded_graph(grid_side=48, seed=3)
+    graphs.append((n, s, d))
+    s4, d4 = random_graph(2500, 4000, 4)
+    graphs.append((2500, s4, d4))
+    batches = []
+    rng = np.random.default_rng(11)
+    for n, s, d in graphs:
+        bl = []
+        for _ in range(5):
+            ki, kd = int(rng.integers(10, 400)), int(rng.integers(10, 200))
+            pick = rng.integers(0, len(s), kd)
+            bl.append((rng.integers(0, n, ki).astype(np.int32), rng.integers(0, n, ki).astype(np.int32),
+                       s[pick].astype(np.int32), d[pick].astype(np.int32)))
+        batches.append(bl)
+    return graphs, batches
+
+
+def run_server(graphs, batches, slots, mixed):
+    sv = Server(num_slots=slots, hbm_budget_bytes=8 << 30)
+    sids = [sv.add_graph(Graph.from_edges(n, s, d)) for n, s, d in graphs]
+    counts = {}
+    if mixed:
+        rids = []
+        for j in range(len(batches[0])):
+            for k, sid in enumerate(sids):
+                rids.append((k, j, sv.submit(sid, *batches[k][j])))
+        for k, j, rid in rids:
+            r = sv.wait(rid)
+            assert r["status"] == 0
+            counts[(k, j)] = r["num_sccs"]
+    else:
+        for k, sid in enumerate(sids):
+            for j, b in enumerate(batches[k]):
+                r = sv.wait(sv.submit(sid, *b))
+                assert r["status"] == 0
+                counts[(k, j)] = r["num_sccs"]
+    sv.drain()
+    labels = [sv.labels(sid) for sid in sids]
+    stats = sv.stats()
+    sv.free()
+    return counts, labels, stats
+
+
+def test_alone_equals_mixed_equals_oracle(gpu):
+    graphs, batches = sessions_and_batches()
+    c_alone, l_alone, st_alone = run_server(graphs, batches, slots=1, mixed=False)
+    c_mix, l_mix, st_mix = run_server(graphs, batches, slots=4, mixed=True)
+    assert c_alone == c_mix
+    for a, b in zip(l_alone, l_mix):
+        assert np.array_equal(a, b)
+    for (n, s, d), bl, lab in zip(graphs, batches, l_mix):
+        for b in bl:
+            s, d = apply_batch(s, d, *b)
+        csr = O.build_csr(n, s, d)
+        assert np.array_equal(lab, O.tarjan_canonical(csr[0], csr[1]))
+    assert st_mix["completed"] == sum(len(b) for b in batches) and st_mix["rejected"] == 0
+    assert st_mix["max_inflight"] >= 2            # requests of different sessions overlapped
+    assert 0 < st_mix["p50_ms"] <= st_mix["p99_ms"]
+
+
+def test_admission_by_hbm_budget(gpu):
+    n, s, d, _ = seeded_graph(rmat_scale=10, edge_factor=4, seed=5)
+    sv = Server(num_slots=2, hbm_budget_bytes=8 << 20)     # 8 MiB
+    sid = sv.add_graph(Graph.from_edges(n, s, d))
+    rng = np.random.default_rng(0)
+    small = sv.wait(sv.submit(sid, rng.integers(0, n, 50), rng.integers(0, n, 50)))
+    assert small["status"] == 0
+    big = sv.wait(sv.submit(sid, rng.integers(0, n, 200000), rng.integers(0, n, 200000)))
+    assert big["status"] == 3                               # SCC_ERR_OOM: never fits
+    st = sv.stats()
+    assert st["rejected"] == 1 and st["completed"] == 2
+    with pytest.raises(Exception):
+        sv.add_graph(Graph.generate(rmat_scale=16, edge_factor=8, seed=1))   # larger than the budget left
+    sv.free()
