@@ -36,6 +36,7 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     "c2": dict(rmat_scale=24, edge_factor=16, grid_side=4096, seed=2024),
     "rmat24": dict(rmat_scale=24, edge_factor=16, seed=2024),
+    "c3": dict(rmat_scale=24, edge_factor=16, num_cycles=1000, cycle_min=3, cycle_max=100000, seed=2024),
     "c1": dict(rmat_scale=16, edge_factor=8, seed=42),
     # smaller cases of the same shapes, for profiler captures
     "rmat22": dict(rmat_scale=22, edge_factor=16, seed=2024),
@@ -45,6 +46,7 @@ WORKLOADS = {
 CPU_SAMPLES = {
     "c2": dict(rmat_scale=20, edge_factor=16, grid_side=1024, seed=2024),
     "rmat24": dict(rmat_scale=20, edge_factor=16, seed=2024),
+    "c3": dict(rmat_scale=20, edge_factor=16, num_cycles=63, cycle_min=3, cycle_max=100000, seed=2024),
     "c1": dict(rmat_scale=16, edge_factor=8, seed=42),
     "rmat22": dict(rmat_scale=18, edge_factor=16, seed=2024),
     "grid4096": dict(grid_side=1024, seed=2024),
@@ -52,6 +54,7 @@ CPU_SAMPLES = {
 WORKLOAD_NAMES = {
     "c2": "R-MAT s24 ef16 (a=.57,b=.19,c=.19) U 4096x4096 randomly oriented grid (+5% bidirectional)",
     "rmat24": "R-MAT s24 ef16 (a=.57,b=.19,c=.19)",
+    "c3": "R-MAT s24 ef16 (a=.57,b=.19,c=.19) + 1,000 planted directed cycles, lengths log-uniform [3, 100,000]",
     "c1": "R-MAT s16 ef8 (a=.57,b=.19,c=.19)",
     "rmat22": "R-MAT s22 ef16 (a=.57,b=.19,c=.19)",
     "grid4096": "4096x4096 randomly oriented grid (+5% bidirectional)",
@@ -65,6 +68,15 @@ def measured_peak_gbs():
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def measured_peak_tflops():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
 
 
 class ClockSampler:
@@ -150,6 +162,28 @@ def run_reference(args, workload):
     sample = f"{WORKLOAD_NAMES[workload]} scaled to " + json.dumps(kw) + f": n={n} m={s.size}"
     return gteps, ms, dict(value=gteps, unit="GTEPS", cores=threads if kind == "reference" else 1, kind=kind,
                            sample=sample, ms=ms)
+
+
+def train_pivot_model(device):
+    """The learned pivot proposer, trained as the configuration asks: records of
+    plain runs on 64 seeded R-MAT graphs of scales 18-22 (ef16), then Adam on the
+    device.  Returns (model, info)."""
+    from dynamicgraphs_scc_b200 import Graph, PivotModel, collect_pivot_records
+    t0 = time.perf_counter()
+    xs, ts = [], []
+    for sd in range(64):
+        g = Graph.generate(rmat_scale=18 + sd % 5, edge_factor=16, seed=7000 + sd, device=device)
+        x, t = collect_pivot_records(g, capacity=1 << 17, per_round=4096)
+        xs.append(x); ts.append(t); g.free()
+    x = np.concatenate(xs); t = np.concatenate(ts)
+    t1 = time.perf_counter()
+    m = PivotModel(seed=0, device=device)
+    losses = m.train(x, t, epochs=12, batch=1024, lr=2e-3, seed=0)
+    t2 = time.perf_counter()
+    info = {"graphs": 64, "records": int(t.size), "target_mean": round(float(t.mean()), 5),
+            "target_var": round(float(t.var()), 6), "epochs": 12, "final_loss": round(float(losses[-1]), 6),
+            "collect_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2)}
+    return m, info
 
 
 BATCH = dict(num_graphs=4096, n_min=1024, n_max=65536, mean_degree=6.0, rmat_fraction=0.3, seed=4096)
@@ -346,51 +380,68 @@ def main():
     from dynamicgraphs_scc_b200 import Graph, State, capi
 
     kw = WORKLOADS[args.workload]
+    learned = args.workload == "c3"            # the learned-pivot configuration
+    model, model_info = (train_pivot_model(local_rank) if learned else (None, None))
     g = Graph.generate(**kw, device=local_rank)
     n, m = g.num_nodes(), g.num_edges()
     st = State(g)
+    if model is not None:
+        st.set_pivot_model(model)
+    pivot_mode = 1 if learned else 0
     stream = torch.cuda.ExternalStream(st.stream(), device=local_rank)
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    for _ in range(args.warmup):
-        st.reset()
-        st.run(2)
-    st.synchronize()
+    def timed(mode, sampler=None):
+        """W untimed steps, then K steps bracketed by barrier + synchronize and
+        CUDA events on the state's stream; max over ranks."""
+        for _ in range(args.warmup):
+            st.reset()
+            st.run(2, mode)
+        st.synchronize()
+        if sampler is not None:
+            sampler.start()
+        barrier()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        kernels = 0
+        phase = []
+        capi.call("scc_state_profile", st.handle, 1)   # time the dominant kernel's launches on this stream
+        ev0.record(stream)
+        for _ in range(args.steps):
+            st.reset()
+            stats = st.run(2, mode)
+            kernels += stats["kernels_launched"] + 3
+            phase.append(stats)
+        ev1.record(stream)
+        st.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        clocks = sampler.stop() if sampler is not None else None
+        l_ms, l_launch, l_items, l_edges = C.c_double(), C.c_int64(), C.c_int64(), C.c_int64()
+        capi.call("scc_state_profile_read", st.handle, C.byref(l_ms), C.byref(l_launch), C.byref(l_items),
+                  C.byref(l_edges))
+        capi.call("scc_state_profile", st.handle, 0)
+        ms = ev0.elapsed_time(ev1) / args.steps
+        if dist is not None:
+            t = torch.tensor([ms], device=f"cuda:{local_rank}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, kernels, phase, clocks, (l_ms, l_launch, l_items, l_edges)
 
-    sampler = ClockSampler(local_rank)
-    sampler.start()
-    barrier()
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    kernels = 0
-    per_step = []
-    phase = []
-    capi.call("scc_state_profile", st.handle, 1)   # time the dominant kernel's launches on this stream
-    ev0.record(stream)
-    for _ in range(args.steps):
-        st.reset()
-        stats = st.run(2)
-        kernels += stats["kernels_launched"] + 3
-        per_step.append(stats["ms_total"])
-        phase.append(stats)
-    ev1.record(stream)
-    st.synchronize()
-    torch.cuda.synchronize()
-    barrier()
-    clocks = sampler.stop()
-    l_ms, l_launch, l_items, l_edges = C.c_double(), C.c_int64(), C.c_int64(), C.c_int64()
-    capi.call("scc_state_profile_read", st.handle, C.byref(l_ms), C.byref(l_launch), C.byref(l_items),
-              C.byref(l_edges))
-    capi.call("scc_state_profile", st.handle, 0)
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    plain = None
+    if learned:                                 # the plain-pivot form on the same GPU, for the comparison
+        p_ms, _, p_phase, _, _ = timed(0)
+        plain_labels = st.canonical_labels() if rank == 0 else None
+        plain = {"value": round(m * world / (p_ms * 1e-3) / 1e9, 4), "unit": "GTEPS", "ms_per_step": round(p_ms, 4),
+                 "fb_rounds": p_phase[-1]["fb_rounds"], "traversal_steps": p_phase[-1]["traversal_steps"]}
+    ms, kernels, phase, clocks, ledger = timed(pivot_mode, ClockSampler(local_rank))
+    l_ms, l_launch, l_items, l_edges = ledger
+    if learned and rank == 0:
+        plain["labels_equal_learned"] = bool(np.array_equal(plain_labels, st.canonical_labels()))
     total_edges = m * world
     gteps = total_edges / (ms * 1e-3) / 1e9
 
@@ -427,7 +478,7 @@ def main():
         capi.call("scc_graph_upload_csr", g.handle, hb.data_ptr(), ha.data_ptr(), hrb.data_ptr(), hra.data_ptr(),
                   st.stream())
         st.reset()
-        st.run(2)
+        st.run(2, pivot_mode)
         capi.call("scc_canonical_labels", st.handle, C.cast(labels.data_ptr(), C.POINTER(C.c_int32)))
         e1.record(stream)
         st.synchronize()
@@ -462,8 +513,9 @@ def main():
         "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32", "data": "synthetic (seeded generator, same shapes as the benchmark configuration)",
         "config": {"workload": WORKLOAD_NAMES[args.workload], "params": kw, "n": n, "m": m, "method": 2,
-                   "pivot": "max in*out degree", "parallelism": f"replicas x{world}",
-                   "l2": "inputs (CSR+transpose) > L2; no flush"},
+                   "pivot": ("learned (MLP 8-64-64-1, BF16 weights, re-ranks the in*out candidates)" if learned
+                             else "max in*out degree"),
+                   "parallelism": f"replicas x{world}", "l2": "inputs (CSR+transpose) > L2; no flush"},
         "roofline": kernel_roofline,
         "roofline_step": {"bound": "hbm", "scope": "whole step (16M+20N+8 algorithmic bytes)",
                           "achieved": round(achieved, 2), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
@@ -478,6 +530,20 @@ def main():
         "stats": {k: last[k] for k in ("num_sccs", "first_scc_size", "trimmed_first", "trimmed_second",
                                         "num_wcc_classes", "traversal_steps")},
     }
+    if learned:
+        line["metric"] = "SCC GTEPS, learned pivot (plain pivot beside it)"
+        line["plain_pivot"] = plain
+        line["learned_speedup"] = round(plain["ms_per_step"] / ms, 4)
+        line["pivot_model"] = model_info
+        # the inference kernel alone: tensor-core roofline (2 x 4,672 useful FLOPs per vertex scored)
+        rows = 1 << 22
+        mlp_ms = model.bench_inference(rows, 20)
+        tflops = 2 * 4672 * rows / (mlp_ms * 1e-3) / 1e12
+        tpeak, tkind = measured_peak_tflops()
+        line["mlp_roofline"] = {"bound": "tensor", "kernel": "k_mlp_score_tc", "rows": rows,
+                                "ms_per_launch": round(mlp_ms, 4), "achieved": round(tflops, 3), "peak": tpeak,
+                                "peak_kind": tkind, "unit": "TFLOP/s", "frac": round(tflops / tpeak, 5),
+                                "rows_per_s": round(rows / (mlp_ms * 1e-3), 1)}
     print(json.dumps(line))
 
 

@@ -33,6 +33,7 @@ CU_SOURCES = [
     "scc_update.cu",
     "scc_tune.cu",
     "scc_server.cu",
+    "scc_mlp.cu",
 ]
 
 

@@ -93,6 +93,7 @@ class BatchParams(C.Structure):
 _P = C.c_void_p
 _I32P = C.POINTER(C.c_int32)
 _I64P = C.POINTER(C.c_int64)
+_F32P = C.POINTER(C.c_float)
 
 # name -> argtypes (all return int status unless listed in _RESTYPES)
 _SIGS = {
@@ -182,6 +183,19 @@ _SIGS = {
     "scc_gen_batch_edges_host": [C.POINTER(BatchParams), _I32P, _I32P, C.c_int64, _I64P],
     "scc_gen_batch_graph": [C.POINTER(BatchParams), C.c_int, C.c_int, C.POINTER(_P)],
     "scc_graph_subgraph": [_P, C.c_int32, C.c_int32, C.POINTER(_P)],
+    "scc_pivot_model_create": [C.c_int, C.c_uint64, C.POINTER(_P)],
+    "scc_pivot_model_free": [_P],
+    "scc_pivot_model_get_params": [_P, _F32P],
+    "scc_pivot_model_set_params": [_P, _F32P],
+    "scc_pivot_model_save": [_P, C.c_char_p],
+    "scc_pivot_model_load": [C.c_int, C.c_char_p, C.POINTER(_P)],
+    "scc_pivot_model_forward": [_P, _F32P, C.c_int64, C.c_int, _F32P],
+    "scc_pivot_model_bench": [_P, C.c_int64, C.c_int, C.POINTER(C.c_double)],
+    "scc_pivot_model_loss_grad": [_P, _F32P, _F32P, C.c_int64, _F32P, _F32P],
+    "scc_pivot_model_train": [_P, _F32P, _F32P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_uint64, _F32P],
+    "scc_state_set_pivot_model": [_P, _P],
+    "scc_state_pivot_log": [_P, C.c_int64, C.c_int32],
+    "scc_state_pivot_records": [_P, _F32P, _F32P, _I32P, _I32P, C.c_int64, _I64P],
 }
 _RESTYPES = {"scc_status_string": C.c_char_p, "scc_last_error": C.c_char_p, "scc_version": C.c_int}
 
@@ -220,6 +234,13 @@ def i32p(a: np.ndarray | None):
         return None
     assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"], "need contiguous int32"
     return a.ctypes.data_as(_I32P)
+
+
+def f32p(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"], "need contiguous float32"
+    return a.ctypes.data_as(_F32P)
 
 
 def out_i32() -> C.c_int32:

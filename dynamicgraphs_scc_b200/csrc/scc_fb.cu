@@ -14,6 +14,7 @@
 // direction, visited bits in a byte per vertex), and a classify pass gives
 // each class the reference's outcome.  A single class (curr_color) is the
 // global step.
+#include <algorithm>
 #include "scc_round.cuh"
 
 // Reset the per-colour pivot slots of the classes present and total the
@@ -32,6 +33,7 @@ __global__ void k_slot_reset(RoundArgs a, int reset_slots) {
         if (reset_slots) {
             a.slot_key[c + 1] = 0ull;
             a.slot_pivot[c + 1] = SCC_NIL_NODE;
+            a.slot_count[c + 1] = 0;
         }
     }
     for (int o = 16; o > 0; o >>= 1) deg += __shfl_down_sync(0xFFFFFFFFu, deg, o);
@@ -47,20 +49,6 @@ __global__ void k_pivot_key(RoundArgs a) {
         unsigned long long k = pivot_key(a.begin, a.r_begin, v);
         if (k > a.slot_key[c + 1]) atomicMax(a.slot_key + c + 1, k);
     }
-}
-
-// The pivot of each class claims two fresh colours and seeds the frontier.
-__device__ __forceinline__ void seed_pivot(const RoundArgs& a, int32_t v, int32_t c, int32_t* q) {
-    a.slot_pivot[c + 1] = v;
-    int32_t old = atomicAdd(a.ctr + CTR_NEXT_COLOR, 2);
-    if ((int64_t)old + 4 >= a.colour_cap) { atomicExch(a.ctr + CTR_ERROR, SCC_DEVERR_COLOR_OVERFLOW); }
-    a.slot_fw[c + 1] = old + 1;
-    a.slot_bw[c + 1] = old + 2;
-    a.mark[v] = 3;
-    int32_t pos = atomicAdd(a.ctr + CTR_QLEN, 2);
-    q[pos] = v;
-    q[pos + 1] = v | (1 << DIR_SHIFT);
-    atomicAdd(a.ctr + CTR_NUM_CLASSES, 1);
 }
 
 __global__ void k_pivot_pick(RoundArgs a, int32_t* q) {
@@ -112,13 +100,14 @@ static RoundArgs round_args(const scc_graph* g, scc_state* s) {
     a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin; a.r_node_idx = g->r_node_idx;
     a.color = s->color; a.scc = s->scc; a.mark = s->mark;
     a.slot_key = s->slot_key; a.slot_pivot = s->slot_pivot; a.slot_fw = s->slot_fw; a.slot_bw = s->slot_bw;
+    a.slot_count = s->slot_count;
     a.colour_cap = s->colour_cap;
     a.ctr = s->ctr;
     a.live = s->live; a.live_count = s->live_count;
     a.only_color = 0; a.use_only = 0;
-    a.pivot_score = nullptr;
     a.huge_deg = s->tune.huge_deg;
     a.async_keep = s->tune.async_keep;
+    a.async_bail = std::max<int32_t>(8 * s->tune.async_max, 1 << 16);
     return a;
 }
 
@@ -147,8 +136,12 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
     } else {
         k_pivot_key<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
         SCC_LAUNCHED(s);
-        k_pivot_pick<<<blocks, SCC_THREADS, 0, s->stream>>>(a, s->qa);
-        SCC_LAUNCHED(s);
+        const bool learned = s->pivot_mode == SCC_PIVOT_LEARNED && s->pivot_model;
+        if (learned || s->log_cap > 0) SCC_TRY(scc_impl_pivot_prepare(g, s, a, learned, s->qa));
+        if (!learned) {
+            k_pivot_pick<<<blocks, SCC_THREADS, 0, s->stream>>>(a, s->qa);
+            SCC_LAUNCHED(s);
+        }
     }
     SCC_TRY(scc_sync_counters(s));
     if (s->h_ctr[CTR_ERROR]) SCC_TRY(scc_check_device_error(s));

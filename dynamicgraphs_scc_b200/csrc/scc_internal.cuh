@@ -57,7 +57,7 @@ enum {
     CTR_NUM_CLASSES,
     CTR_SPARE0,
     CTR_SPARE1,
-    CTR_SPARE2,
+    CTR_ABAIL,           // asynchronous drain: hand the frontier back to level steps
     CTR_SPARE3,
     CTR_SPARE4,
     CTR_EDGES = 16,      // u64 (slots 16-17): edges of the next top-down frontier
@@ -117,8 +117,21 @@ struct scc_state {
     std::vector<int32_t> wq_colors;
     std::vector<int32_t> wq_counts;
 
-    // learned pivot model (optional)
-    void* pivot_model = nullptr;
+    // learned pivot (scc_mlp.cu)
+    scc_pivot_model* pivot_model = nullptr;  // attached model (not owned)
+    int pivot_mode = SCC_PIVOT_DEGREE;       // mode of the run in progress
+    bool cnt_valid = false;                  // cnt_out/cnt_in hold the first peel's residue
+    int32_t* pivot_cand = nullptr;           // [n] candidates of the learned choice (vertex ids)
+    float* pivot_score = nullptr;            // [n] their scores
+    void* pivot_x = nullptr;                 // [n] their BF16 feature rows (16 B each)
+    // pivot logging (training records)
+    int64_t log_cap = 0;
+    int32_t log_per_round = 0;
+    uint32_t log_salt = 0;
+    float* log_x = nullptr;                  // [log_cap][8]
+    int32_t* log_v = nullptr;                // [log_cap]
+    int32_t* log_size = nullptr;             // [log_cap]
+    int32_t* log_ctr = nullptr;              // records appended (may exceed log_cap)
 
     cudaEvent_t ev[16];
     bool events = false;
@@ -158,6 +171,7 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
 int scc_impl_wcc(const scc_graph* g, scc_state* s);
 int scc_impl_uf_split(const scc_graph* g, scc_state* s, int32_t* num_classes);
 bool scc_trace_on();
+void scc_impl_pivot_release(scc_state* s);   // frees the learned-pivot and logging buffers
 int scc_impl_resolve_all(const scc_graph* g, scc_state* s);
 int scc_impl_get_live_host(scc_state* s, std::vector<int32_t>& out);
 int scc_impl_count_colour(scc_state* s, int32_t color, int32_t* count);

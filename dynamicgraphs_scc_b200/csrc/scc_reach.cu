@@ -24,6 +24,7 @@
 //    end.  Every wait is bounded: past its limit a warp records
 //    SCC_DEVERR_WAIT_LIMIT and returns, and the host reports SCC_ERR_TIMEOUT.
 #include <stdlib.h>
+#include <algorithm>
 #include "scc_round.cuh"
 
 // switch points come from the state's tunables (scc_tuning)
@@ -402,8 +403,10 @@ __global__ void __launch_bounds__(REACH_THREADS) k_reach_async(RoundArgs a, int3
     int32_t* tail = a.ctr + CTR_ATAIL;
     int32_t* work = a.ctr + CTR_AWORK;
     int32_t* err = a.ctr + CTR_ERROR;
+    int32_t* bail = a.ctr + CTR_ABAIL;
     LocalPush push{sbuf[wid], sbeg[wid], send[wid], 0, 0, q, tail, work, qcap, err, a.async_keep};
     int idle = 0;
+    uint32_t iter = 0;
     int32_t last_work = -1;
     long long my_edges = 0;     // per lane
     long long my_items = 0;     // warp-uniform
@@ -422,11 +425,12 @@ __global__ void __launch_bounds__(REACH_THREADS) k_reach_async(RoundArgs a, int3
             if (got == 0) {
                 ++idle;
                 if ((idle & 7) == 1) {
-                    int32_t w = 1, e = 0;
-                    if (lane == 0) { w = ld_volatile(work); e = ld_volatile(err); }
+                    int32_t w = 1, e = 0, bl = 0;
+                    if (lane == 0) { w = ld_volatile(work); e = ld_volatile(err); bl = ld_volatile(bail); }
                     w = __shfl_sync(0xFFFFFFFFu, w, 0);
                     e = __shfl_sync(0xFFFFFFFFu, e, 0);
-                    if (w == 0 || e != 0) break;
+                    bl = __shfl_sync(0xFFFFFFFFu, bl, 0);
+                    if (w == 0 || e != 0 || bl != 0) break;
                     // the limit bounds a stall, not a long traversal: progress elsewhere resets it
                     if (w != last_work) { last_work = w; idle = 1; }
                 }
@@ -463,8 +467,24 @@ __global__ void __launch_bounds__(REACH_THREADS) k_reach_async(RoundArgs a, int3
         expand_warp_async(a, lane < k, it, ib, ie, push, &my_edges);
         my_items += k;
         int32_t delta = push.pushed - k;
-        if (lane == 0 && delta != 0) atomicAdd(work, delta);
         push.pushed = 0;
+        if ((++iter & 7) == 0) {
+            // every 8th iteration: read back the outstanding work; a frontier that
+            // has grown wide is handed back to the level-synchronous kernels,
+            // which expand wide frontiers far better than one queue
+            int32_t stop = 0;
+            if (lane == 0) {
+                int32_t w = atomicAdd(work, delta) + delta;
+                if (w > a.async_bail) atomicExch(bail, 1);
+                stop = ld_volatile(bail);
+            }
+            if (__shfl_sync(0xFFFFFFFFu, stop, 0)) {
+                push.spill(0);
+                break;
+            }
+        } else if (lane == 0 && delta != 0) {
+            atomicAdd(work, delta);
+        }
         // keep one iteration's worth (this warp's own continuation), share the rest
         if (push.count > push.keep) push.spill(push.keep);
     }
@@ -539,6 +559,8 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
             init[CTR_AWORK - CTR_AHEAD] = qlen;
             SCC_CUDA(cudaMemcpyAsync(s->ctr + CTR_AHEAD, init, sizeof(init), cudaMemcpyHostToDevice, s->stream));
             SCC_TRY(scc_zero_counters(s, CTR_ASYNC_ITEMS, 4));
+            SCC_TRY(scc_zero_counters(s, CTR_ABAIL, 1));
+            a.async_bail = std::max<int32_t>(8 * s->tune.async_max, 1 << 16);
             if (s->ledger_on) SCC_CUDA(cudaEventRecord(s->lev[0], s->stream));
             k_reach_async<<<async_blocks(s->device, s->tune.async_blocks_per_sm), REACH_THREADS, 0, s->stream>>>(a, s->aq, qcap);
             SCC_LAUNCHED(s);
@@ -562,7 +584,20 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
                 SCC_CUDA(cudaMemsetAsync(s->aq, 0xFF, sizeof(int32_t) * (size_t)qcap, s->stream));
                 return scc_check_device_error(s);
             }
-            return SCC_OK;
+            if (!s->h_ctr[CTR_ABAIL]) return SCC_OK;
+            // the frontier grew wide: its unexpanded items are aq[head, tail)
+            // (every warp spilled its own before leaving); continue level by level
+            int32_t h = s->h_ctr[CTR_AHEAD], t = s->h_ctr[CTR_ATAIL];
+            qlen = t - h;
+            if (qlen > 0) {
+                SCC_CUDA(cudaMemcpyAsync(qin, s->aq + h, sizeof(int32_t) * (size_t)qlen, cudaMemcpyDeviceToDevice,
+                                         s->stream));
+                SCC_CUDA(cudaMemsetAsync(s->aq + h, 0xFF, sizeof(int32_t) * (size_t)qlen, s->stream));
+            }
+            narrow = 0;
+            bottom_up = false;
+            if (scc_trace_on()) fprintf(stderr, "[scc] reach async handed back %d items\n", qlen);
+            continue;
         } else {
             SCC_TRY(scc_zero_counters(s, CTR_QLEN, 1));
             SCC_TRY(scc_zero_counters(s, CTR_SPARE4, 1));

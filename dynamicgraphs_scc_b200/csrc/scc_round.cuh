@@ -11,14 +11,15 @@ struct RoundArgs {
     const int32_t* begin; const int32_t* node_idx; const int32_t* r_begin; const int32_t* r_node_idx;
     int32_t* color; int32_t* scc; uint8_t* mark;
     unsigned long long* slot_key; int32_t* slot_pivot; int32_t* slot_fw; int32_t* slot_bw;
+    int32_t* slot_count;        // members per colour (learned-pivot feature)
     int64_t colour_cap;
     int32_t* ctr;
     const int32_t* live; int32_t live_count;
     int32_t only_color;   // used when use_only
     int32_t use_only;
-    const float* pivot_score;   // optional learned score per vertex (nullptr = degree rule)
     int32_t huge_deg;           // top-down items above this degree go edge-parallel
     int32_t async_keep;         // items a warp keeps before sharing in the asynchronous drain
+    int32_t async_bail;         // outstanding items at which the drain hands back to level steps
 };
 
 __device__ __forceinline__ uint32_t pivot_hash(uint32_t v) {
@@ -36,6 +37,27 @@ __device__ __forceinline__ unsigned long long pivot_key(const int32_t* __restric
     if (prod > 0xFFFFFFFEull) prod = 0xFFFFFFFEull;
     return ((prod + 1ull) << 32) | pivot_hash((uint32_t)v);
 }
+
+// The pivot of class c claims two fresh colours and seeds the frontier with
+// its FW and BW items.
+__device__ __forceinline__ void seed_pivot(const RoundArgs& a, int32_t v, int32_t c, int32_t* q) {
+    a.slot_pivot[c + 1] = v;
+    int32_t old = atomicAdd(a.ctr + CTR_NEXT_COLOR, 2);
+    if ((int64_t)old + 4 >= a.colour_cap) { atomicExch(a.ctr + CTR_ERROR, SCC_DEVERR_COLOR_OVERFLOW); }
+    a.slot_fw[c + 1] = old + 1;
+    a.slot_bw[c + 1] = old + 2;
+    a.mark[v] = 3;
+    int32_t pos = atomicAdd(a.ctr + CTR_QLEN, 2);
+    q[pos] = v;
+    q[pos + 1] = v | (1 << DIR_SHIFT);
+    atomicAdd(a.ctr + CTR_NUM_CLASSES, 1);
+}
+
+// Learned-pivot work of a round (scc_mlp.cu), after the degree keys are in
+// slot_key: class sizes, training records when logging is on, and, when
+// `learned`, the pivot of every class chosen by the network among the class's
+// degree candidates and seeded into q (instead of the degree pick).
+int scc_impl_pivot_prepare(const scc_graph* g, scc_state* s, RoundArgs& a, bool learned, int32_t* q);
 
 // Claim w for direction `dir` inside colour c; true if this thread claimed it.
 __device__ __forceinline__ bool visit(const RoundArgs& a, int32_t w, int32_t c, int dir) {

@@ -140,7 +140,11 @@ extern "C" int scc_run(const scc_graph* g, scc_state* s, int method, int pivot_m
     int k0 = s->kernels;
     int64_t steps0 = s->traversal_steps;
     int32_t rounds0 = s->fb_rounds;
+    if (pivot_mode == SCC_PIVOT_LEARNED)
+        SCC_REQUIRE(s->pivot_model, SCC_ERR_INVALID, "learned pivots need a model (scc_state_set_pivot_model)");
+    s->pivot_mode = pivot_mode;
     int rc = run_method(g, s, method, &st);
+    s->pivot_mode = SCC_PIVOT_DEGREE;
     if (rc != SCC_OK) return rc;
     SCC_CUDA(cudaStreamSynchronize(s->stream));
     SCC_TRY(scc_check_device_error(s));

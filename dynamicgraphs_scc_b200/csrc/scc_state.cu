@@ -209,6 +209,7 @@ extern "C" int scc_state_reset(scc_state* s) {
     SCC_CUDA(cudaStreamSynchronize(s->stream));
     s->live_count = -1;
     s->fresh = true;
+    s->cnt_valid = false;
     s->wq_colors.clear();
     s->wq_counts.clear();
     s->kernels = 0;
@@ -224,6 +225,7 @@ extern "C" int scc_state_free(scc_state* s) {
     cudaFree(s->ctr);
     if (s->h_ctr) cudaFreeHost(s->h_ctr);
     cudaFree(s->slot_key); cudaFree(s->slot_pivot); cudaFree(s->slot_fw); cudaFree(s->slot_bw); cudaFree(s->slot_count);
+    scc_impl_pivot_release(s);
     if (s->events) {
         for (int i = 0; i < 16; ++i) cudaEventDestroy(s->ev[i]);
         for (int i = 0; i < 2; ++i) cudaEventDestroy(s->lev[i]);

@@ -297,6 +297,7 @@ static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     }
     *trimmed = (int32_t)total;
     s->fresh = false;
+    s->cnt_valid = true;
     return SCC_OK;
 }
 

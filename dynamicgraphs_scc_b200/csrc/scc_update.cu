@@ -283,13 +283,14 @@ static RoundArgs update_round_args(const scc_graph* g, scc_state* s) {
     a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin; a.r_node_idx = g->r_node_idx;
     a.color = s->color; a.scc = s->scc; a.mark = s->mark;
     a.slot_key = s->slot_key; a.slot_pivot = s->slot_pivot; a.slot_fw = s->slot_fw; a.slot_bw = s->slot_bw;
+    a.slot_count = s->slot_count;
     a.colour_cap = s->colour_cap;
     a.ctr = s->ctr;
     a.live = s->live; a.live_count = s->live_count;
     a.only_color = 0; a.use_only = 1;
-    a.pivot_score = nullptr;
     a.huge_deg = s->tune.huge_deg;
     a.async_keep = s->tune.async_keep;
+    a.async_bail = std::max<int32_t>(8 * s->tune.async_max, 1 << 16);
     return a;
 }
 

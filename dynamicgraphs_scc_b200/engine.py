@@ -13,7 +13,7 @@ import ctypes as C
 import numpy as np
 
 from . import capi
-from .capi import SccError, call, i32p
+from .capi import SccError, call, f32p, i32p
 
 METHOD_BASELINE = 0
 METHOD_GLOBAL_FB = 1
@@ -376,6 +376,26 @@ class State:
         call("scc_insert_idea1", self._g(), self.handle, int(s.size), i32p(s), i32p(d), C.byref(st))
         return st.as_dict()
 
+    # -- learned pivot ---------------------------------------------------------------------------
+    def set_pivot_model(self, model: "PivotModel | None") -> None:
+        call("scc_state_set_pivot_model", self.handle, model.handle if model is not None else None)
+        self._model = model            # keep the model alive while attached
+
+    def pivot_log(self, capacity: int, per_round: int = 4096) -> None:
+        """Record training samples in the following runs (capacity 0 stops and drops them)."""
+        call("scc_state_pivot_log", self.handle, int(capacity), int(per_round))
+
+    def pivot_records(self):
+        """(x [k, 8] float32, t [k] float32, v [k] int32, class_size [k] int32) after a run."""
+        k = C.c_int64()
+        call("scc_state_pivot_records", self.handle, None, None, None, None, 0, C.byref(k))
+        n = k.value
+        x = np.empty((n, 8), np.float32); t = np.empty(n, np.float32)
+        v = np.empty(n, np.int32); cs = np.empty(n, np.int32)
+        if n:
+            call("scc_state_pivot_records", self.handle, f32p(x), f32p(t), i32p(v), i32p(cs), n, C.byref(k))
+        return x[:k.value], t[:k.value], v[:k.value], cs[:k.value]
+
     def free(self) -> None:
         if self._h is not None:
             capi.lib().scc_state_free(self._h)
@@ -386,6 +406,99 @@ class State:
             self.free()
         except Exception:
             pass
+
+
+MLP_FEATURES = 8
+MLP_PARAMS = 4801
+
+
+class PivotModel:
+    """The learned pivot proposer: 8 -> 64 -> 64 -> 1 ReLU network on the device
+    (BF16 weights, FP32 accumulation), trained by the engine's own kernels."""
+
+    def __init__(self, seed: int = 0, device: int = 0, handle=None):
+        if handle is None:
+            handle = C.c_void_p()
+            call("scc_pivot_model_create", device, int(seed), C.byref(handle))
+        self._h = handle
+
+    @classmethod
+    def load(cls, path: str, device: int = 0) -> "PivotModel":
+        h = C.c_void_p()
+        call("scc_pivot_model_load", device, path.encode(), C.byref(h))
+        return cls(handle=h)
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise SccError(capi.SCC_ERR_STATE, "PivotModel", "model was freed")
+        return self._h
+
+    def save(self, path: str) -> None:
+        call("scc_pivot_model_save", self.handle, path.encode())
+
+    def params(self) -> np.ndarray:
+        p = np.empty(MLP_PARAMS, np.float32)
+        call("scc_pivot_model_get_params", self.handle, f32p(p))
+        return p
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(np.asarray(p, np.float32))
+        assert p.size == MLP_PARAMS
+        call("scc_pivot_model_set_params", self.handle, f32p(p))
+
+    def forward(self, x, tensor_cores: bool = True) -> np.ndarray:
+        x = np.ascontiguousarray(np.asarray(x, np.float32).reshape(-1, MLP_FEATURES))
+        y = np.empty(x.shape[0], np.float32)
+        call("scc_pivot_model_forward", self.handle, f32p(x), x.shape[0], int(bool(tensor_cores)), f32p(y))
+        return y
+
+    def bench_inference(self, count: int, iters: int = 10) -> float:
+        """Device ms of one tensor-core inference launch over `count` resident rows."""
+        ms = C.c_double()
+        call("scc_pivot_model_bench", self.handle, int(count), int(iters), C.byref(ms))
+        return ms.value
+
+    def loss_grad(self, x, t):
+        x = np.ascontiguousarray(np.asarray(x, np.float32).reshape(-1, MLP_FEATURES))
+        t = np.ascontiguousarray(np.asarray(t, np.float32))
+        g = np.empty(MLP_PARAMS, np.float32)
+        loss = C.c_float()
+        call("scc_pivot_model_loss_grad", self.handle, f32p(x), f32p(t), x.shape[0], f32p(g), C.byref(loss))
+        return float(loss.value), g
+
+    def train(self, x, t, epochs: int = 20, batch: int = 1024, lr: float = 2e-3, seed: int = 0) -> np.ndarray:
+        x = np.ascontiguousarray(np.asarray(x, np.float32).reshape(-1, MLP_FEATURES))
+        t = np.ascontiguousarray(np.asarray(t, np.float32))
+        losses = np.empty(max(epochs, 1), np.float32)
+        call("scc_pivot_model_train", self.handle, f32p(x), f32p(t), x.shape[0], int(epochs), int(batch),
+             float(lr), int(seed), f32p(losses))
+        return losses[:epochs]
+
+    def free(self) -> None:
+        if self._h is not None:
+            capi.lib().scc_pivot_model_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def collect_pivot_records(graph: Graph, capacity: int = 1 << 20, per_round: int = 4096,
+                          method: int = METHOD_GLOBAL_WCC_FB):
+    """One plain (degree-pivot) run of `graph` with logging on; returns its records (x, t)."""
+    st = State(graph)
+    try:
+        st.pivot_log(capacity, per_round)
+        st.reset()
+        st.run(method, PIVOT_DEGREE)
+        x, t, _, _ = st.pivot_records()
+        return x, t
+    finally:
+        st.free()
 
 
 class Server:

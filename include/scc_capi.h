@@ -348,6 +348,54 @@ int scc_server_labels(scc_server* sv, int32_t session, int32_t* labels);
 int scc_server_session_graph(scc_server* sv, int32_t session, scc_graph** g);
 int scc_server_free(scc_server* sv);
 
+/* ---- learned pivot proposer (no counterpart in the reference, whose pivot is the
+ * first vertex of the colour, src/scc_color.cc:64-93) ------------------------------------
+ * An 8 -> 64 -> 64 -> 1 ReLU network (4,801 parameters; parameter order W1[8][64],
+ * b1[64], W2[64][64], b2[64], w3[64], b3) scores the vertices of every class; with
+ * SCC_PIVOT_LEARNED each class pivots on its highest-scoring vertex.  Weights are
+ * used in BF16 with FP32 accumulation (tensor cores for inference).  A pivot only
+ * changes the speed of a run, never its labels.
+ * Features per vertex (log1p-scaled, rounded to BF16): out-degree, in-degree, their
+ * product, live out- and in-neighbours after the first peel (trim residue), size of
+ * the vertex's class, mean degree of its first 4 out-neighbours, largest degree of
+ * its first 4 in-neighbours. */
+#define SCC_MLP_FEATURES 8
+#define SCC_MLP_HIDDEN 64
+#define SCC_MLP_PARAMS 4801
+typedef struct scc_pivot_model scc_pivot_model;
+/* Uniform He initialisation from a seed. */
+int scc_pivot_model_create(int device, uint64_t seed, scc_pivot_model** out);
+int scc_pivot_model_free(scc_pivot_model* m);
+int scc_pivot_model_get_params(const scc_pivot_model* m, float* params);      /* FP32 master copy */
+int scc_pivot_model_set_params(scc_pivot_model* m, const float* params);
+int scc_pivot_model_save(const scc_pivot_model* m, const char* path);
+int scc_pivot_model_load(int device, const char* path, scc_pivot_model** out);
+/* Scores of count host feature rows.  tensor_cores = 1: the inference kernel
+ * (tcgen05 MMA, BF16 activations); 0: FP32 activations on the CUDA cores. */
+int scc_pivot_model_forward(const scc_pivot_model* m, const float* x, int64_t count, int tensor_cores, float* y);
+/* Device time of one inference launch over count resident rows (CUDA events,
+ * mean of iters launches after one warm-up): the tensor-core kernel alone. */
+int scc_pivot_model_bench(const scc_pivot_model* m, int64_t count, int iters, double* ms_per_launch);
+/* Mean squared error over count rows and its gradient w.r.t. the parameters as
+ * used (BF16 weights, FP32 activations) -- the training kernels' gradient. */
+int scc_pivot_model_loss_grad(const scc_pivot_model* m, const float* x, const float* t, int64_t count,
+                              float* grad, float* loss);
+/* Adam (beta 0.9 / 0.999) on shuffled mini-batches, on the device.
+ * epoch_loss (may be NULL) receives the mean loss of each epoch. */
+int scc_pivot_model_train(scc_pivot_model* m, const float* x, const float* t, int64_t count, int epochs,
+                          int batch, float lr, uint64_t seed, float* epoch_loss);
+/* Attach a model to a state (NULL detaches); runs with SCC_PIVOT_LEARNED need one. */
+int scc_state_set_pivot_model(scc_state* s, scc_pivot_model* m);
+/* Pivot logging for training: each FW-BW round of the following runs records
+ * the features of about per_round sampled vertices of the classes it pivots,
+ * up to capacity records in all (capacity 0 turns logging off and drops them). */
+int scc_state_pivot_log(scc_state* s, int64_t capacity, int32_t per_round);
+/* After a run: the records (features x[count][8], vertex v, size of its class at
+ * the time) and targets t = log1p(|SCC(v)|) / log1p(class size), the share of
+ * the class that v resolves as a pivot.  count receives the number written. */
+int scc_state_pivot_records(scc_state* s, float* x, float* t, int32_t* v, int32_t* class_size, int64_t cap,
+                            int64_t* count);
+
 /* One-call convenience: host CSR in, canonical labels out (H2D + run + D2H). */
 int scc_decompose_csr(int32_t n, int32_t m, const int32_t* begin, const int32_t* node_idx,
                       const int32_t* r_begin, const int32_t* r_node_idx, int method, int device,

@@ -1,7 +1,8 @@
 """CPU oracle for the SCC engine -- TEST INFRASTRUCTURE ONLY.
 
 Loads two native libraries built by oracle/Makefile:
-  build/liboracle.so  -- the C restatement of the reference algorithms (scc_oracle.c);
+  build/liboracle.so  -- the C restatement of the reference algorithms (scc_oracle.c) and of
+                         the learned pivot network, its gradient and features (mlp_oracle.c);
   _ref/libscc_ref.so  -- the reference's own OpenMP engine compiled from its sources
                          plus ref_harness.cc (optional: absent if never built).
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this.
@@ -21,6 +22,8 @@ REF_CLI = os.path.join(HERE, "_ref", "scc")
 _I32P = C.POINTER(C.c_int32)
 _U8P = C.POINTER(C.c_uint8)
 _I64P = C.POINTER(C.c_int64)
+_F32P = C.POINTER(C.c_float)
+_F64P = C.POINTER(C.c_double)
 _lib = None
 _ref = None
 
@@ -56,6 +59,16 @@ def lib():
         L.orc_fw_bw.restype = C.c_int64
         L.orc_choose_pivot.argtypes = [C.c_int32, _I32P, _I32P, _I32P, C.c_int32]
         L.orc_choose_pivot.restype = C.c_int32
+        L.orc_bf16.argtypes = [C.c_float]
+        L.orc_bf16.restype = C.c_float
+        L.orc_mlp_forward.argtypes = [_F32P, _F32P, C.c_int64, C.c_int, _F64P]
+        L.orc_mlp_forward.restype = None
+        L.orc_mlp_loss_grad.argtypes = [_F32P, _F32P, _F32P, C.c_int64, _F64P]
+        L.orc_mlp_loss_grad.restype = C.c_double
+        L.orc_mlp_loss.argtypes = [_F64P, _F32P, _F32P, C.c_int64]
+        L.orc_mlp_loss.restype = C.c_double
+        L.orc_pivot_features.argtypes = [_I32P, _I32P, _I32P, _I32P, _I32P, _I32P, C.c_int32, C.c_int32, _F32P]
+        L.orc_pivot_features.restype = None
         _lib = L
     return _lib
 
@@ -198,3 +211,70 @@ def ref_tarjan(csr):
     if rc != 0:
         raise RuntimeError("reference Tarjan failed")
     return canonical(out[:n]), ms.value
+
+
+# ---------------------------------------------------------------- learned pivot network (mlp_oracle.c)
+MLP_PARAMS = 4801
+
+
+def _f32(a):
+    return np.ascontiguousarray(np.asarray(a, np.float32))
+
+
+def bf16(x):
+    """Round float32 values to BF16 (nearest, ties to even), numpy restatement."""
+    x = _f32(x)
+    u = x.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    out = u.astype(np.uint32).view(np.float32)
+    return np.where(np.isnan(x), x, out)
+
+
+def bf16_scalar(v: float) -> float:
+    return float(lib().orc_bf16(v))
+
+
+def mlp_forward(params, x, bf16_acts=False):
+    p = _f32(params); xx = _f32(x).reshape(-1, 8)
+    y = np.empty(xx.shape[0], np.float64)
+    lib().orc_mlp_forward(p.ctypes.data_as(_F32P), xx.ctypes.data_as(_F32P), xx.shape[0], int(bf16_acts),
+                          y.ctypes.data_as(_F64P))
+    return y
+
+
+def mlp_loss_grad(params, x, t):
+    p = _f32(params); xx = _f32(x).reshape(-1, 8); tt = _f32(t)
+    g = np.empty(MLP_PARAMS, np.float64)
+    loss = lib().orc_mlp_loss_grad(p.ctypes.data_as(_F32P), xx.ctypes.data_as(_F32P), tt.ctypes.data_as(_F32P),
+                                   xx.shape[0], g.ctypes.data_as(_F64P))
+    return float(loss), g
+
+
+def mlp_loss(params64, x, t):
+    """Loss at double parameters taken as given (no BF16 rounding)."""
+    p = np.ascontiguousarray(np.asarray(params64, np.float64)); xx = _f32(x).reshape(-1, 8); tt = _f32(t)
+    return float(lib().orc_mlp_loss(p.ctypes.data_as(_F64P), xx.ctypes.data_as(_F32P), tt.ctypes.data_as(_F32P),
+                                    xx.shape[0]))
+
+
+def pivot_features(csr, v, class_size, cnt_out=None, cnt_in=None):
+    b, a, rb, ra = csr
+    f = np.empty(8, np.float32)
+    lib().orc_pivot_features(_p(b), _p(a), _p(rb), _p(ra), _p(cnt_out), _p(cnt_in), int(v), int(class_size),
+                             f.ctypes.data_as(_F32P))
+    return f
+
+
+def trim_residue(csr, scc_after_trim):
+    """Live out/in neighbours (self-loops excluded) of every vertex after the
+    first Trim1 fixpoint: the engine's trim-residue features."""
+    b, a, rb, ra = csr
+    n = b.size - 1
+    live = scc_after_trim < 0
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(b))
+    ok = live[a] & (a != src)
+    cnt_out = np.bincount(src[ok], minlength=n).astype(np.int32)
+    rsrc = np.repeat(np.arange(n, dtype=np.int64), np.diff(rb))
+    ok = live[ra] & (ra != rsrc)
+    cnt_in = np.bincount(rsrc[ok], minlength=n).astype(np.int32)
+    return cnt_out, cnt_in

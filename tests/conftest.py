@@ -19,9 +19,7 @@ def _ensure_built():
     from dynamicgraphs_scc_b200 import build
     build.build()
     oracle_so = os.path.join(ROOT, "oracle", "build", "liboracle.so")
-    if not os.path.exists(oracle_so):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), os.path.join(ROOT, "oracle", "build", "liboracle.so")],
-                       check=True, capture_output=True)
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), oracle_so], check=True, capture_output=True)
 
 
 _ensure_built()

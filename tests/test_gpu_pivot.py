@@ -1,0 +1,214 @@
+"""GPU: the learned pivot proposer.  Inference (tensor-core and CUDA-core
+forward), the training kernels' gradient, training itself, the logged records
+and features are checked against the CPU oracle; runs in learned mode must give
+exactly the labels of the plain method (Tarjan)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from dynamicgraphs_scc_b200 import Graph, PivotModel, SccError, State, collect_pivot_records
+from dynamicgraphs_scc_b200.engine import METHOD_GLOBAL_WCC_FB, PIVOT_DEGREE, PIVOT_LEARNED
+from tests.helpers import seeded_graph
+
+pytestmark = pytest.mark.gpu
+
+
+def random_params(seed, scale=0.3):
+    rng = np.random.default_rng(seed)
+    return O.bf16((rng.standard_normal(O.MLP_PARAMS) * scale).astype(np.float32))
+
+
+def random_features(seed, n):
+    rng = np.random.default_rng(seed)
+    return O.bf16(rng.uniform(0, 8, (n, 8)).astype(np.float32))
+
+
+@pytest.mark.parametrize("count", [1, 127, 128, 1000, 200003])
+def test_tensor_core_forward_matches_oracle(gpu, count):
+    """tcgen05 inference: BF16 operands, FP32 accumulation; the oracle rounds
+    inputs and the first hidden layer to BF16 the same way."""
+    m = PivotModel(seed=1)
+    p = random_params(5)
+    m.set_params(p)
+    x = random_features(count, count)
+    y = m.forward(x, tensor_cores=True)
+    ref = O.mlp_forward(p, x, bf16_acts=True)
+    err = np.abs(y - ref) / (1.0 + np.abs(ref))
+    # tolerance: FP32 accumulation order, plus an occasional one-ulp BF16
+    # rounding difference of a hidden unit that sits on a rounding boundary
+    assert err.max() < 1e-2, err.max()
+    assert np.median(err) < 1e-5, np.median(err)
+    m.free()
+
+
+def test_cuda_core_forward_matches_oracle(gpu):
+    m = PivotModel(seed=1)
+    p = random_params(6)
+    m.set_params(p)
+    x = random_features(9, 3001)
+    y = m.forward(x, tensor_cores=False)
+    ref = O.mlp_forward(p, x, bf16_acts=False)
+    np.testing.assert_allclose(y, ref, rtol=1e-4, atol=1e-4 * (1 + np.abs(ref).max()))
+    m.free()
+
+
+def test_gradient_matches_oracle(gpu):
+    """The training kernels' gradient (fused forward + backward, shared-memory
+    reductions, atomics across blocks) against the oracle's double gradient."""
+    m = PivotModel(seed=2)
+    p = random_params(8, 0.2)
+    m.set_params(p)
+    rng = np.random.default_rng(4)
+    x = random_features(10, 1000)
+    t = rng.uniform(0, 1, 1000).astype(np.float32)
+    loss, g = m.loss_grad(x, t)
+    loss_ref, g_ref = O.mlp_loss_grad(p, x, t)
+    assert abs(loss - loss_ref) <= 1e-4 * max(1.0, loss_ref)
+    scale = np.abs(g_ref).max()
+    assert np.abs(g - g_ref).max() <= 1e-4 * scale + 1e-7, (np.abs(g - g_ref).max(), scale)
+    m.free()
+
+
+def test_training_fits_a_teacher(gpu):
+    teacher = random_params(21, 0.15)
+    x = random_features(22, 20000)
+    t = O.mlp_forward(teacher, x).astype(np.float32)
+    t = (t - t.mean()) / (t.std() + 1e-6)
+    m = PivotModel(seed=3)
+    losses = m.train(x, t, epochs=30, batch=512, lr=2e-3, seed=1)
+    assert np.all(np.isfinite(losses))
+    assert losses[-1] < 0.2 * losses[0], losses
+    # the trained parameters give the oracle the same loss the device reported
+    p = m.params()
+    assert abs(O.mlp_loss(O.bf16(p).astype(np.float64), x, t) - m.loss_grad(x, t)[0]) < 1e-3
+    m.free()
+
+
+def test_save_load_roundtrip(gpu, tmp_path):
+    m = PivotModel(seed=4)
+    path = str(tmp_path / "pivot.bin")
+    m.save(path)
+    m2 = PivotModel.load(path)
+    assert np.array_equal(m.params(), m2.params())
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(b"not a model")
+    with pytest.raises(SccError):
+        PivotModel.load(str(bad))
+    m.free(); m2.free()
+
+
+def test_records_features_and_targets_match_oracle(gpu):
+    n, s, d, csr = seeded_graph(rmat_scale=11, edge_factor=6, grid_side=40, seed=3)
+    g = Graph.from_edges(n, s, d)
+    st = State(g)
+    st.pivot_log(1 << 16, per_round=1 << 16)          # every vertex of every pivoted class
+    st.reset()
+    st.run(METHOD_GLOBAL_WCC_FB, PIVOT_DEGREE)
+    x, t, v, cs = st.pivot_records()
+    assert len(v) > 100
+    # features: trim residue after the first Trim1 fixpoint, class size as logged
+    color = np.full(n, -1, np.int32); scc = np.full(n, -1, np.int32)
+    O.trim1_fixpoint(csr, color, scc)
+    cnt_out, cnt_in = O.trim_residue(csr, scc)
+    ref = np.stack([O.pivot_features(csr, int(vi), int(ci), cnt_out, cnt_in) for vi, ci in zip(v, cs)])
+    # log1pf of the device and of the C library may differ in the last FP32 bit,
+    # which can move a BF16 rounding by one step (2^-8 relative)
+    diff = np.abs(x - ref) / np.maximum(np.abs(ref), 1e-30)
+    assert np.mean(x == ref) > 0.99
+    assert diff.max() <= 2.0 ** -7
+    # the global round's class is every vertex the first peel left
+    live_after_trim = int(np.sum(scc < 0))
+    assert cs.max() == live_after_trim
+    # targets from the final SCC sizes (Tarjan)
+    lab = O.tarjan_canonical(csr[0], csr[1])
+    sizes = np.bincount(lab, minlength=n)
+    t_ref = np.log1p(sizes[lab[v]].astype(np.float32)) / np.log1p(cs.astype(np.float32))
+    np.testing.assert_allclose(t, t_ref, rtol=1e-5)
+    st.free()
+
+
+def _quick_model(seed=0):
+    xs, ts = [], []
+    for sd in range(3):
+        g = Graph.generate(rmat_scale=12, edge_factor=8, grid_side=32, seed=100 + sd)
+        x, t = collect_pivot_records(g, capacity=1 << 16, per_round=2048)
+        xs.append(x); ts.append(t)
+    m = PivotModel(seed=seed)
+    m.train(np.concatenate(xs), np.concatenate(ts), epochs=10, batch=512, lr=2e-3)
+    return m
+
+
+@pytest.mark.parametrize("kw", [
+    dict(rmat_scale=12, edge_factor=8, seed=1),
+    dict(grid_side=64, seed=2),
+    dict(rmat_scale=13, edge_factor=8, num_cycles=40, cycle_min=3, cycle_max=2000, seed=3),
+    dict(rmat_scale=11, edge_factor=4, grid_side=48, seed=4),
+])
+def test_learned_pivot_labels_exact(gpu, kw):
+    m = _quick_model()
+    n, s, d, csr = seeded_graph(**kw)
+    g = Graph.from_edges(n, s, d)
+    st = State(g)
+    st.set_pivot_model(m)
+    st.reset()
+    r = st.run(METHOD_GLOBAL_WCC_FB, PIVOT_LEARNED)
+    assert r["pivot_mode"] == PIVOT_LEARNED
+    assert np.array_equal(st.canonical_labels(), O.tarjan_canonical(csr[0], csr[1]))
+    st.free(); m.free()
+
+
+def test_learned_mode_needs_a_model(gpu):
+    g = Graph.generate(rmat_scale=8, edge_factor=4, seed=1)
+    st = State(g)
+    st.reset()
+    with pytest.raises(SccError):
+        st.run(METHOD_GLOBAL_WCC_FB, PIVOT_LEARNED)
+    st.reset()
+    st.run(METHOD_GLOBAL_WCC_FB, PIVOT_DEGREE)       # the state stays usable
+    st.free()
+
+
+def _spearman(a, b):
+    from scipy.stats import spearmanr          # ties get average ranks
+    return float(spearmanr(a, b).correlation)
+
+
+def test_trained_network_gain_over_degree_rule(gpu):
+    """What training buys: on held-out records of graphs with many SCCs per
+    class (R-MAT U oriented grid), the trained network ranks vertices by the
+    share of their class they resolve as pivots better than the plain rule's
+    score (log in*out) and better than the untrained network; a learned run
+    gives the plain run's labels.  End-to-end speed is measured by bench.py
+    (workload c3) and reported, not asserted."""
+    xs, ts = [], []
+    for sd in range(6):
+        g = Graph.generate(rmat_scale=14, edge_factor=8, grid_side=128, seed=300 + sd)
+        x, t = collect_pivot_records(g, capacity=1 << 17, per_round=8192)
+        xs.append(x); ts.append(t); g.free()
+    x_tr, t_tr = np.concatenate(xs[:4]), np.concatenate(ts[:4])
+    x_te, t_te = np.concatenate(xs[4:]), np.concatenate(ts[4:])
+    assert t_te.std() > 0.05                           # these records carry contrast
+    untrained = PivotModel(seed=9)
+    trained = PivotModel(seed=9)
+    losses = trained.train(x_tr, t_tr, epochs=25, batch=512, lr=2e-3, seed=2)
+    assert losses[-1] < losses[0]
+    rho_trained = _spearman(trained.forward(x_te), t_te)
+    rho_untrained = abs(_spearman(untrained.forward(x_te), t_te))
+    rho_degree = _spearman(x_te[:, 2], t_te)           # feature 2 = log1p(in*out), the plain rule's order
+    assert rho_trained > rho_degree + 0.05, (rho_trained, rho_degree)
+    assert rho_trained > rho_untrained + 0.05, (rho_trained, rho_untrained)
+    # held-out mean squared error below the constant predictor's
+    mse = float(np.mean((trained.forward(x_te, tensor_cores=False) - t_te) ** 2))
+    assert mse < float(np.var(t_te)), (mse, float(np.var(t_te)))
+    n, s, d, csr = seeded_graph(rmat_scale=13, edge_factor=8, grid_side=96, seed=77)
+    g = Graph.from_edges(n, s, d)
+    st = State(g)
+    st.set_pivot_model(trained)
+    st.reset()
+    st.run(METHOD_GLOBAL_WCC_FB, PIVOT_LEARNED)
+    learned = st.canonical_labels()
+    st.reset()
+    st.run(METHOD_GLOBAL_WCC_FB, PIVOT_DEGREE)
+    assert np.array_equal(learned, st.canonical_labels())
+    assert np.array_equal(learned, O.tarjan_canonical(csr[0], csr[1]))
+    st.free(); trained.free(); untrained.free()

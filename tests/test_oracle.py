@@ -118,3 +118,67 @@ def test_fw_bw_restatement_finds_pivot_scc():
     assert size == int((lab == lab[p]).sum())
     assert np.all(scc[lab == lab[p]] == p)
     assert fw == int((color == 0).sum()) and bw == int((color == 1).sum())
+
+
+# ---------------------------------------------------------------- learned pivot network
+def _mlp_case(seed, n=48):
+    rng = np.random.default_rng(seed)
+    p = O.bf16((rng.standard_normal(O.MLP_PARAMS) * 0.3).astype(np.float32))
+    x = O.bf16(rng.uniform(0, 6, (n, 8)).astype(np.float32))
+    t = rng.uniform(0, 1, n).astype(np.float32)
+    return p, x, t
+
+
+def test_bf16_rounding_matches_torch():
+    import torch
+    rng = np.random.default_rng(3)
+    x = np.concatenate([rng.standard_normal(4000).astype(np.float32) * 50,
+                        np.array([0.0, -0.0, 1.0, 1.00390625, 1.0029296875, 65504.0, 3.4e38], np.float32)])
+    ref = torch.from_numpy(x).to(torch.bfloat16).float().numpy()
+    assert np.array_equal(O.bf16(x), ref)
+    assert all(O.bf16_scalar(float(v)) == r for v, r in zip(x[:200], ref[:200]))
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """Pins the oracle's backward pass: central differences of the loss (double
+    parameters, step 1e-6) against the analytic gradient, on the BF16 grid."""
+    p, x, t = _mlp_case(7)
+    loss, g = O.mlp_loss_grad(p, x, t)
+    w = p.astype(np.float64)
+    assert abs(O.mlp_loss(w, x, t) - loss) < 1e-12
+    rng = np.random.default_rng(1)
+    idx = np.concatenate([rng.choice(512, 24, replace=False),                 # W1
+                          512 + rng.choice(64, 8, replace=False),             # b1
+                          576 + rng.choice(4096, 40, replace=False),          # W2
+                          4672 + rng.choice(64, 8, replace=False),            # b2
+                          4736 + rng.choice(64, 8, replace=False), [4800]])   # w3, b3
+    h = 1e-6
+    for i in idx:
+        wp = w.copy(); wp[i] += h
+        wm = w.copy(); wm[i] -= h
+        fd = (O.mlp_loss(wp, x, t) - O.mlp_loss(wm, x, t)) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(g[i]), (int(i), fd, g[i])
+
+
+def test_mlp_oracle_forward_consistent_with_loss():
+    p, x, t = _mlp_case(11)
+    y = O.mlp_forward(p, x)
+    assert abs(np.mean((y - t.astype(np.float64)) ** 2) - O.mlp_loss_grad(p, x, t)[0]) < 1e-12
+    yb = O.mlp_forward(p, x, bf16_acts=True)          # activation rounding moves y only slightly
+    assert np.max(np.abs(yb - y)) < 0.05 * (1 + np.max(np.abs(y)))
+
+
+def test_pivot_features_oracle_known_answer():
+    # 0 -> 1, 0 -> 2, 1 -> 0, 2 -> 0, 3 -> 0: vertex 0 has out-degree 2, in-degree 3
+    n = 4
+    s = np.array([0, 0, 1, 2, 3], np.int32); d = np.array([1, 2, 0, 0, 0], np.int32)
+    csr = O.build_csr(n, s, d)
+    f = O.pivot_features(csr, 0, class_size=3)
+    exp = np.log1p(np.array([2, 3, 6, 2, 3, 3, 0, 0], np.float32))
+    exp[6] = np.float32(np.log1p(1.0))               # out-neighbours 1, 2 have out-degree 1
+    exp[7] = np.float32(np.log1p(1.0))               # in-neighbours 1, 2, 3: in-degrees 1, 1, 0
+    np.testing.assert_allclose(f, O.bf16(exp), rtol=0, atol=0)
+    cnt_out, cnt_in = O.trim_residue(csr, np.array([-1, -1, -1, 3], np.int32))   # vertex 3 trimmed
+    assert list(cnt_out) == [2, 1, 1, 1] and list(cnt_in) == [2, 1, 1, 0]
+    f2 = O.pivot_features(csr, 0, class_size=3, cnt_out=cnt_out, cnt_in=cnt_in)
+    assert f2[4] == O.bf16(np.float32(np.log1p(2.0)))
