@@ -19,21 +19,32 @@
 
 // Reset the per-colour pivot slots of the classes present and total the
 // in+out degree of the vertices this round will traverse (the direction rule
-// of the traversal compares frontier edges against it).
+// of the traversal compares frontier edges against it).  Lanes of a warp that
+// share a class reset its slots once, and a thread skips the class it reset
+// last, so a round over one huge class does not pile stores onto one address.
 __global__ void k_slot_reset(RoundArgs a, int reset_slots) {
     unsigned long long deg = 0;
+    int32_t last = INT32_MIN;
+    const int lane = threadIdx.x & 31;
     int64_t limit = (((int64_t)a.live_count + 31) / 32) * 32;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += (int64_t)gridDim.x * blockDim.x) {
-        if (i >= a.live_count) continue;
-        int32_t v = a.live[i];
-        int32_t c = a.color[v];
-        if (c == SCC_COLOR_DONE || (a.use_only && c != a.only_color)) continue;
-        deg += (unsigned)(__ldg(a.begin + v + 1) - __ldg(a.begin + v)) +
-               (unsigned)(__ldg(a.r_begin + v + 1) - __ldg(a.r_begin + v));
-        if (reset_slots) {
+        int32_t c = SCC_COLOR_DONE;
+        if (i < a.live_count) {
+            int32_t v = a.live[i];
+            c = a.color[v];
+            if (c != SCC_COLOR_DONE && !(a.use_only && c != a.only_color))
+                deg += (unsigned)(__ldg(a.begin + v + 1) - __ldg(a.begin + v)) +
+                       (unsigned)(__ldg(a.r_begin + v + 1) - __ldg(a.r_begin + v));
+            else
+                c = SCC_COLOR_DONE;
+        }
+        if (!reset_slots) continue;
+        unsigned grp = __match_any_sync(0xFFFFFFFFu, c);
+        if (c != SCC_COLOR_DONE && lane == __ffs(grp) - 1 && c != last) {
             a.slot_key[c + 1] = 0ull;
             a.slot_pivot[c + 1] = SCC_NIL_NODE;
             a.slot_count[c + 1] = 0;
+            last = c;
         }
     }
     for (int o = 16; o > 0; o >>= 1) deg += __shfl_down_sync(0xFFFFFFFFu, deg, o);
@@ -41,13 +52,29 @@ __global__ void k_slot_reset(RoundArgs a, int reset_slots) {
         atomicAdd(reinterpret_cast<unsigned long long*>(a.ctr + CTR_LIVE_EDGES), deg);
 }
 
+// Per-class maximum of the pivot keys.  A warp whose lanes all belong to one
+// class reduces its keys first and issues one atomic.
 __global__ void k_pivot_key(RoundArgs a) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.live_count; i += (int64_t)gridDim.x * blockDim.x) {
-        int32_t v = a.live[i];
-        int32_t c = a.color[v];
-        if (c == SCC_COLOR_DONE || (a.use_only && c != a.only_color)) continue;
-        unsigned long long k = pivot_key(a.begin, a.r_begin, v);
-        if (k > a.slot_key[c + 1]) atomicMax(a.slot_key + c + 1, k);
+    const int lane = threadIdx.x & 31;
+    int64_t limit = (((int64_t)a.live_count + 31) / 32) * 32;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t c = SCC_COLOR_DONE;
+        unsigned long long k = 0ull;
+        if (i < a.live_count) {
+            int32_t v = a.live[i];
+            c = a.color[v];
+            if (c == SCC_COLOR_DONE || (a.use_only && c != a.only_color)) c = SCC_COLOR_DONE;
+            else k = pivot_key(a.begin, a.r_begin, v);
+        }
+        unsigned grp = __match_any_sync(0xFFFFFFFFu, c);
+        if (grp == 0xFFFFFFFFu) {
+            for (int o = 16; o > 0; o >>= 1) {
+                unsigned long long other = __shfl_xor_sync(0xFFFFFFFFu, k, o);
+                k = other > k ? other : k;
+            }
+            if (lane != 0) continue;
+        }
+        if (c != SCC_COLOR_DONE && k > a.slot_key[c + 1]) atomicMax(a.slot_key + c + 1, k);
     }
 }
 

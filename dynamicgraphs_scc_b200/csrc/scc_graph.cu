@@ -197,6 +197,7 @@ int scc_impl_build_graph_from_device_edges(int32_t n, int64_t m, const int32_t* 
     int64_t m1 = 0, m2 = 0;
     int s = build_side(n, m, d_src, d_dst, flags, st, &g->begin, &g->node_idx, &m1);
     if (s == SCC_OK) s = build_side(n, m, d_dst, d_src, flags, st, &g->r_begin, &g->r_node_idx, &m2);
+    if (flags & SCC_BUILD_NO_SELF_LOOPS) g->self_loops = 0;
     cudaStreamDestroy(st);
     if (s != SCC_OK) { scc_graph_free(g); return s; }
     g->m = m1;
@@ -294,6 +295,7 @@ extern "C" int scc_graph_upload_csr(scc_graph* g, const int32_t* begin, const in
     SCC_CUDA(cudaSetDevice(g->device));
     cudaStream_t st = (cudaStream_t)stream;
     size_t nb = sizeof(int32_t) * ((size_t)g->n + 1), mb = sizeof(int32_t) * (size_t)g->m;
+    g->self_loops = -1;                      // new contents: count again when needed
     SCC_CUDA(cudaMemcpyAsync(g->begin, begin, nb, cudaMemcpyHostToDevice, st));
     SCC_CUDA(cudaMemcpyAsync(g->r_begin, r_begin, nb, cudaMemcpyHostToDevice, st));
     if (g->m > 0) {

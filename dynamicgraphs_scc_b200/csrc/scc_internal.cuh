@@ -40,6 +40,7 @@ struct scc_graph {
     int32_t* r_node_idx = nullptr;// [m]    in-neighbours        (gm_graph::r_node_idx)
     bool owns = true;
     bool async_arrays = false;    // arrays come from cudaMallocAsync (after an update)
+    mutable int64_t self_loops = -1;  // edges u->u in the CSR; -1 = not counted yet
 };
 
 // Device counters block (one allocation, mirrored to pinned host memory).

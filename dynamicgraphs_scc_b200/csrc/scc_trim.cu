@@ -174,14 +174,42 @@ __device__ __forceinline__ int32_t self_run(const int32_t* __restrict__ off, con
     return lo - first;
 }
 
+// Live-degree counts; the self-loop runs are looked up only when the graph has
+// self-loops (graphs built without them skip the adjacency reads entirely).
 __global__ void k_count_init(const int32_t* __restrict__ begin, const int32_t* __restrict__ node_idx,
                              const int32_t* __restrict__ r_begin, const int32_t* __restrict__ r_node_idx, int32_t n,
-                             int32_t* __restrict__ cnt_out, int32_t* __restrict__ cnt_in) {
+                             int has_self, int32_t* __restrict__ cnt_out, int32_t* __restrict__ cnt_in) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         int32_t v = (int32_t)i;
-        cnt_out[v] = (__ldg(begin + v + 1) - __ldg(begin + v)) - self_run(begin, node_idx, v);
-        cnt_in[v] = (__ldg(r_begin + v + 1) - __ldg(r_begin + v)) - self_run(r_begin, r_node_idx, v);
+        int32_t co = __ldg(begin + v + 1) - __ldg(begin + v), ci = __ldg(r_begin + v + 1) - __ldg(r_begin + v);
+        if (has_self) {
+            co -= self_run(begin, node_idx, v);
+            ci -= self_run(r_begin, r_node_idx, v);
+        }
+        cnt_out[v] = co;
+        cnt_in[v] = ci;
     }
+}
+
+// Self-loops of the CSR (each appears once in the out-lists).
+__global__ void k_count_self(const int32_t* __restrict__ begin, const int32_t* __restrict__ node_idx, int32_t n,
+                             unsigned long long* __restrict__ total) {
+    unsigned long long c = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        c += (unsigned)self_run(begin, node_idx, (int32_t)i);
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(total, c);
+}
+
+static int count_self_loops(const scc_graph* g, scc_state* s) {
+    if (g->self_loops >= 0) return SCC_OK;
+    SCC_TRY(scc_zero_counters(s, CTR_EDGES, 2));
+    k_count_self<<<scc_blocks(g->n), SCC_THREADS, 0, s->stream>>>(g->begin, g->node_idx, g->n,
+                                                                   reinterpret_cast<unsigned long long*>(s->ctr + CTR_EDGES));
+    SCC_LAUNCHED(s);
+    SCC_TRY(scc_sync_counters(s));
+    g->self_loops = (int64_t)*reinterpret_cast<unsigned long long*>(s->h_ctr + CTR_EDGES);
+    return SCC_OK;
 }
 
 struct CountArgs {
@@ -196,75 +224,106 @@ __device__ __forceinline__ bool count_trim(const CountArgs& a, int32_t v) {
     return true;
 }
 
-// Decrement the counts of x's neighbours; trimmed ones go on the stack.
-__device__ void count_cascade(const CountArgs& a, int32_t x0, int32_t& cnt) {
-    int32_t stk[TRIM_STACK];
-    int sp = 0;
-    stk[sp++] = x0;
-    while (sp > 0) {
-        int32_t x = stk[--sp];
-        int32_t ob = __ldg(a.begin + x), oe = __ldg(a.begin + x + 1);
-        int32_t ib = __ldg(a.r_begin + x), ie = __ldg(a.r_begin + x + 1);
-        if ((oe - ob) + (ie - ib) > TRIM_BIG_DEG) {
-            int32_t pos = atomicAdd(a.ctr + CTR_OVERFLOW, 1);
-            a.ovf[pos] = x;
-            continue;
+#define PEEL_Q 256          // per-warp queue of trimmed vertices awaiting expansion
+
+// Expand this warp's queued trimmed vertices, 32 at a time, with their edges
+// spread over the lanes (a warp prefix sum of the degrees; each lane finds the
+// vertex owning its edge by a binary search over the lanes): every trimmed x
+// decrements the live count of each neighbour -- out-neighbours lose an
+// in-neighbour, in-neighbours an out-neighbour -- so a warp issues 32
+// independent atomics per round trip.  A count reaching zero trims that
+// neighbour (the colour CAS makes it happen once), which joins the queue, or
+// the overflow list when the queue is full.
+__device__ void peel_drain(const CountArgs& a, int32_t* wq, int32_t& qn, int32_t& cnt) {
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xFFFFFFFFu;
+    while (qn > 0) {
+        const int32_t take = min(qn, 32);
+        qn -= take;
+        const int32_t x = lane < take ? wq[qn + lane] : -1;
+        __syncwarp();
+        int32_t ob = 0, od = 0, ib = 0, id = 0;
+        if (x >= 0) {
+            ob = __ldg(a.begin + x); od = __ldg(a.begin + x + 1) - ob;
+            ib = __ldg(a.r_begin + x); id = __ldg(a.r_begin + x + 1) - ib;
         }
-        // out-neighbour w loses an in-neighbour; in-neighbour u loses an out-neighbour
-        for (int32_t k = ob; k < oe; ++k) {
-            int32_t w = __ldg(a.node_idx + k);
-            if (w == x) continue;
-            if (atomicSub(a.cnt_in + w, 1) == 1 && count_trim(a, w)) {
-                cnt++;
-                if (sp < TRIM_STACK) stk[sp++] = w;
-                else { int32_t pos = atomicAdd(a.ctr + CTR_OVERFLOW, 1); a.ovf[pos] = w; }
+        const int32_t d = od + id;
+        int32_t incl = d;
+        for (int o = 1; o < 32; o <<= 1) {
+            int32_t t = __shfl_up_sync(full, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int32_t total = __shfl_sync(full, incl, 31);
+        const int32_t excl = incl - d;
+        for (int32_t j0 = 0; j0 < total; j0 += 32) {
+            const int32_t j = j0 + lane;
+            int owner = 0;                                   // largest lane with excl <= j
+            for (int step = 16; step > 0; step >>= 1) {
+                int cand = owner + step;
+                int32_t ev = __shfl_sync(full, excl, cand);
+                if (ev <= j) owner = cand;
             }
-        }
-        for (int32_t k = ib; k < ie; ++k) {
-            int32_t u = __ldg(a.r_node_idx + k);
-            if (u == x) continue;
-            if (atomicSub(a.cnt_out + u, 1) == 1 && count_trim(a, u)) {
-                cnt++;
-                if (sp < TRIM_STACK) stk[sp++] = u;
-                else { int32_t pos = atomicAdd(a.ctr + CTR_OVERFLOW, 1); a.ovf[pos] = u; }
+            const int32_t k = j - __shfl_sync(full, excl, owner);
+            const int32_t ox = __shfl_sync(full, x, owner);
+            const int32_t oob = __shfl_sync(full, ob, owner), ood = __shfl_sync(full, od, owner);
+            const int32_t oib = __shfl_sync(full, ib, owner);
+            int32_t nv = -1;
+            if (j < total) {
+                if (k < ood) {
+                    int32_t w = __ldg(a.node_idx + oob + k);
+                    if (w != ox && atomicSub(a.cnt_in + w, 1) == 1 && count_trim(a, w)) nv = w;
+                } else {
+                    int32_t u = __ldg(a.r_node_idx + oib + (k - ood));
+                    if (u != ox && atomicSub(a.cnt_out + u, 1) == 1 && count_trim(a, u)) nv = u;
+                }
+            }
+            const unsigned bal = __ballot_sync(full, nv >= 0);
+            if (bal) {
+                const int32_t r = __popc(bal & ((1u << lane) - 1u)), nn = __popc(bal);
+                if (qn + nn <= PEEL_Q) {
+                    if (nv >= 0) wq[qn + r] = nv;
+                    qn += nn;
+                } else {
+                    int32_t base = 0;
+                    if (lane == 0) base = atomicAdd(a.ctr + CTR_OVERFLOW, nn);
+                    base = __shfl_sync(full, base, 0);
+                    if (nv >= 0) a.ovf[base + r] = nv;
+                }
+                cnt += nv >= 0;
+                __syncwarp();
             }
         }
     }
 }
 
-__global__ void k_count_peel(CountArgs a, int32_t n) {
-    int32_t cnt = 0;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    int64_t limit = (((int64_t)n + 31) / 32) * 32;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += stride) {
+// Sweep (items == NULL): every vertex with a zero count is trimmed and
+// expanded.  List (items != NULL): expand trimmed vertices that overflowed a
+// queue.  Each warp drains its queue after every 32 vertices.
+__global__ void __launch_bounds__(SCC_THREADS) k_count_peel(CountArgs a, int32_t n, const int32_t* __restrict__ items) {
+    __shared__ int32_t queues[SCC_THREADS / 32][PEEL_Q];
+    const int lane = threadIdx.x & 31;
+    int32_t* wq = queues[threadIdx.x >> 5];
+    int32_t qn = 0, cnt = 0;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += nwarps * 32) {
+        const int64_t i = base + lane;
+        int32_t x = -1;
         if (i < n) {
-            int32_t v = (int32_t)i;
-            if ((__ldcg(a.cnt_out + v) == 0 || __ldcg(a.cnt_in + v) == 0) && count_trim(a, v)) {
-                cnt++;
-                count_cascade(a, v, cnt);
+            if (items) {
+                x = items[i];
+            } else {
+                int32_t v = (int32_t)i;
+                if ((__ldcg(a.cnt_out + v) == 0 || __ldcg(a.cnt_in + v) == 0) && count_trim(a, v)) {
+                    x = v;
+                    cnt++;
+                }
             }
         }
-    }
-    block_count_add(a.ctr + CTR_COUNT, cnt);
-}
-
-// Overflow: one warp per trimmed high-degree (or deep-chain) vertex.
-__global__ void k_count_overflow(CountArgs a, const int32_t* __restrict__ items, int32_t n_items) {
-    int lane = threadIdx.x & 31;
-    int32_t cnt = 0;
-    int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t wi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; wi < n_items; wi += wstride) {
-        int32_t x = items[wi];
-        int32_t ob = __ldg(a.begin + x), oe = __ldg(a.begin + x + 1);
-        for (int32_t k = ob + lane; k < oe; k += 32) {
-            int32_t w = __ldg(a.node_idx + k);
-            if (w != x && atomicSub(a.cnt_in + w, 1) == 1 && count_trim(a, w)) { cnt++; count_cascade(a, w, cnt); }
-        }
-        int32_t ib = __ldg(a.r_begin + x), ie = __ldg(a.r_begin + x + 1);
-        for (int32_t k = ib + lane; k < ie; k += 32) {
-            int32_t u = __ldg(a.r_node_idx + k);
-            if (u != x && atomicSub(a.cnt_out + u, 1) == 1 && count_trim(a, u)) { cnt++; count_cascade(a, u, cnt); }
-        }
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, x >= 0);
+        if (x >= 0) wq[qn + __popc(bal & ((1u << lane) - 1u))] = x;    // qn == 0 here
+        qn += __popc(bal);
+        __syncwarp();
+        peel_drain(a, wq, qn, cnt);
     }
     block_count_add(a.ctr + CTR_COUNT, cnt);
 }
@@ -277,10 +336,11 @@ static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     a.ovf = s->qa; a.ctr = s->ctr;
     SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
     SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
+    SCC_TRY(count_self_loops(g, s));
     k_count_init<<<scc_blocks(n), SCC_THREADS, 0, s->stream>>>(g->begin, g->node_idx, g->r_begin, g->r_node_idx, n,
-                                                               s->cnt_out, s->cnt_in);
+                                                               g->self_loops > 0 ? 1 : 0, s->cnt_out, s->cnt_in);
     SCC_LAUNCHED(s);
-    k_count_peel<<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, n);
+    k_count_peel<<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, n, nullptr);
     SCC_LAUNCHED(s);
     int64_t total = 0;
     for (int round = 0; round < 1000000; ++round) {
@@ -291,8 +351,7 @@ static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
         SCC_CUDA(cudaMemcpyAsync(s->qb, s->qa, sizeof(int32_t) * (size_t)novf, cudaMemcpyDeviceToDevice, s->stream));
         SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
         SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
-        k_count_overflow<<<scc_blocks((int64_t)novf * 32, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, s->qb,
-                                                                                                          novf);
+        k_count_peel<<<scc_blocks(novf, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, novf, s->qb);
         SCC_LAUNCHED(s);
     }
     *trimmed = (int32_t)total;

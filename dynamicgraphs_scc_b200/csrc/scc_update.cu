@@ -354,6 +354,7 @@ extern "C" int scc_update_batch(scc_graph* g, scc_state* s, int64_t n_ins, const
     if (rc != SCC_OK) { cudaFreeAsync(nb, st); cudaFreeAsync(na, st); return rc; }
     release_graph_arrays(g, st);
     g->begin = nb; g->node_idx = na; g->r_begin = nrb; g->r_node_idx = nra; g->m = m1;
+    g->self_loops = -1;
     g->async_arrays = true;
     SCC_CUDA(cudaEventRecord(s->ev[9], st));
 
@@ -462,6 +463,7 @@ extern "C" int scc_insert_idea1(scc_graph* g, scc_state* s, int64_t n_ins, const
                        &nrb, &nra, &m2));
     release_graph_arrays(g, st);
     g->begin = nb; g->node_idx = na; g->r_begin = nrb; g->r_node_idx = nra; g->m = m1;
+    g->self_loops = -1;
     g->async_arrays = true;
     SCC_TRY(scc_state_reset(s));
     return scc_run(g, s, SCC_METHOD_GLOBAL_WCC_FB, SCC_PIVOT_DEGREE, stats);
