@@ -265,6 +265,8 @@ def bench_serving(args, local_rank):
     b, a, _, _ = g.csr()
     base_src = np.repeat(np.arange(n, dtype=np.int32), np.diff(b)); base_dst = a
     sv = Server(num_slots=4, hbm_budget_bytes=96 << 30, device=local_rank)
+    if args.coalesce > 1:
+        sv.set_coalesce(args.coalesce)
     sid = sv.add_graph(g)
     rng = np.random.default_rng(2022)
     lo, hi = np.log(1e3), np.log(1e6)
@@ -307,7 +309,8 @@ def bench_serving(args, local_rank):
         "data": "synthetic (seeded)",
         "config": {"workload": "R-MAT s22 ef16 base, Poisson(2 ms) arrivals, batch log-uniform [1e3, 1e6], "
                                "70% insert / 30% delete, degree-proportional endpoints",
-                   "batches": len(results), "n": n, "m_before": m0, "m_after": int(cb[-1]), "slots": 4},
+                   "batches": len(results), "n": n, "m_before": m0, "m_after": int(cb[-1]), "slots": 4,
+                   "coalesce": args.coalesce, "device_updates": st["groups"]},
         "latency_ms": {"p50": round(st["p50_ms"], 3), "p99": round(st["p99_ms"], 3), "max": round(st["max_ms"], 3)},
         "service_ms": {"p50": round(pct(service, 0.5), 3), "p99": round(pct(service, 0.99), 3)},
         "tarjan_checks": {"count": checks, "all_equal": check_ok},
@@ -326,6 +329,7 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5"])
     ap.add_argument("--tune-trials", type=int, default=8)
     ap.add_argument("--batches", type=int, default=200)
+    ap.add_argument("--coalesce", type=int, default=1, help="c5: queued batches of a session composed per update")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

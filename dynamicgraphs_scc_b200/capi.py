@@ -64,7 +64,8 @@ class RequestResult(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_int64), ("rejected", C.c_int64), ("updates", C.c_int64),
                 ("max_inflight", C.c_int64), ("bytes_in_use", C.c_int64), ("p50_ms", C.c_double),
-                ("p99_ms", C.c_double), ("max_ms", C.c_double), ("updates_per_s", C.c_double)]
+                ("p99_ms", C.c_double), ("max_ms", C.c_double), ("updates_per_s", C.c_double),
+                ("groups", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -170,6 +171,7 @@ _SIGS = {
     "scc_server_create": [C.c_int, C.c_int, C.c_int64, C.POINTER(_P)],
     "scc_server_add_graph": [_P, _P, _I32P],
     "scc_server_submit": [_P, C.c_int32, C.c_int64, _I32P, _I32P, C.c_int64, _I32P, _I32P, _I64P],
+    "scc_server_set_coalesce": [_P, C.c_int32, C.c_int64],
     "scc_server_wait": [_P, C.c_int64, C.POINTER(RequestResult)],
     "scc_server_drain": [_P],
     "scc_server_get_stats": [_P, C.POINTER(ServerStats)],

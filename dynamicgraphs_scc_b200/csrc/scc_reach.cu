@@ -368,22 +368,24 @@ __device__ __forceinline__ void expand_warp_async(const RoundArgs& a, bool valid
             p[u] = (j0 + u) < mydeg;
             w[u] = p[u] ? __ldg(adj + b + j0 + u) : 0;
         }
+        // the neighbour's range is loaded with its mark and colour (speculatively:
+        // most neighbours on a narrow frontier are new), so the claim that
+        // follows waits only on the L2-resident mark word
         unsigned mk[4];
         int32_t col[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             mk[u] = p[u] ? (unsigned)*(volatile uint8_t*)(a.mark + w[u]) : bit;
             col[u] = p[u] ? __ldg(a.color + w[u]) : c;
+            wb[u] = p[u] ? __ldg(off + w[u]) : -1;
+            we[u] = p[u] ? __ldg(off + w[u] + 1) : -1;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             p[u] = p[u] && !(mk[u] & bit) && col[u] == c;
-            wb[u] = we[u] = -1;
             if (p[u]) {
                 unsigned sh = (unsigned)(w[u] & 3) * 8u;
                 unsigned old = atomicOr(reinterpret_cast<unsigned*>(a.mark + (w[u] & ~3)), bit << sh);
-                wb[u] = __ldg(off + w[u]);
-                we[u] = __ldg(off + w[u] + 1);
                 p[u] = ((old >> sh) & bit) == 0u;
             }
         }

@@ -11,6 +11,15 @@
 // different sessions therefore overlap on the device.  A request that could
 // never fit the budget is rejected with SCC_ERR_OOM.  Latency = completion -
 // submission (host clock); p50/p99 and updates/s are kept.
+//
+// Coalescing (scc_server_set_coalesce, off by default): when a session's turn
+// comes with several of its requests queued, up to max_requests of them
+// (max_edges edges in all) are composed into one batch and applied by one
+// update, so one CSR merge and one recompute serve them all.  Composition keeps
+// the sequential result exactly: a batch deletes every copy of its deleted
+// pairs and then adds its inserts, so an insert survives the group unless a
+// later batch of the group deletes that pair.  Every request of a group
+// completes with the group's result (the session after the whole group).
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -54,8 +63,72 @@ struct scc_server {
     int64_t next_id = 1;
     std::vector<double> latencies;
     int64_t updates_done = 0, completed = 0, rejected = 0, max_inflight = 0, inflight = 0;
+    int64_t groups = 0;          // updates applied (one per request, or per coalesced group)
+    int32_t coalesce = 1;        // requests per group (1 = off)
+    int64_t coalesce_edges = 0;  // edge cap of a group
     double t_first = -1.0, t_last = 0.0;
 };
+
+// ------------------------------------------------------------------ composition of queued batches
+// Open-addressing map from an edge key (u << 32 | v) to the index of the last
+// batch of the group that deletes it.
+struct LastDelete {
+    std::vector<unsigned long long> keys;
+    std::vector<int32_t> vals;
+    size_t mask = 0;
+    explicit LastDelete(size_t n) {
+        size_t cap = 16;
+        while (cap < 2 * n + 16) cap <<= 1;
+        keys.assign(cap, ~0ull);
+        vals.assign(cap, -1);
+        mask = cap - 1;
+    }
+    static size_t hash(unsigned long long k) {
+        k ^= k >> 33; k *= 0xFF51AFD7ED558CCDull; k ^= k >> 33;
+        return (size_t)k;
+    }
+    void put(unsigned long long k, int32_t v) {
+        for (size_t i = hash(k) & mask;; i = (i + 1) & mask) {
+            if (keys[i] == k || keys[i] == ~0ull) { keys[i] = k; vals[i] = v; return; }
+        }
+    }
+    int32_t get(unsigned long long k) const {
+        for (size_t i = hash(k) & mask;; i = (i + 1) & mask) {
+            if (keys[i] == k) return vals[i];
+            if (keys[i] == ~0ull) return -1;
+        }
+    }
+};
+
+static inline unsigned long long edge_key(int32_t u, int32_t v) {
+    return ((unsigned long long)(uint32_t)u << 32) | (uint32_t)v;
+}
+
+// One batch equivalent to applying grp's batches in order (see the header).
+static void compose_group(const std::vector<ServerRequest*>& grp, std::vector<int32_t>& is, std::vector<int32_t>& id,
+                          std::vector<int32_t>& ds, std::vector<int32_t>& dd) {
+    size_t nd = 0, ni = 0;
+    for (auto* r : grp) { nd += r->del_src.size(); ni += r->ins_src.size(); }
+    LastDelete last(nd);
+    ds.reserve(nd); dd.reserve(nd);
+    for (size_t j = 0; j < grp.size(); ++j) {
+        const ServerRequest* r = grp[j];
+        for (size_t e = 0; e < r->del_src.size(); ++e) {
+            last.put(edge_key(r->del_src[e], r->del_dst[e]), (int32_t)j);
+            ds.push_back(r->del_src[e]);
+            dd.push_back(r->del_dst[e]);
+        }
+    }
+    is.reserve(ni); id.reserve(ni);
+    for (size_t j = 0; j < grp.size(); ++j) {
+        const ServerRequest* r = grp[j];
+        for (size_t e = 0; e < r->ins_src.size(); ++e) {
+            if (nd && last.get(edge_key(r->ins_src[e], r->ins_dst[e])) > (int32_t)j) continue;   // deleted later
+            is.push_back(r->ins_src[e]);
+            id.push_back(r->ins_dst[e]);
+        }
+    }
+}
 
 static double now_ms() {
     using namespace std::chrono;
@@ -75,6 +148,8 @@ static void worker_main(scc_server* sv) {
     for (;;) {
         ServerRequest* r = nullptr;
         ServerSession* ses = nullptr;
+        std::vector<ServerRequest*> grp;
+        int64_t grp_bytes = 0;
         {
             std::unique_lock<std::mutex> lk(sv->mu);
             for (;;) {
@@ -109,37 +184,77 @@ static void worker_main(scc_server* sv) {
                 if (rejected_one) continue;   // the queue changed: scan again
                 sv->cv_work.wait(lk);
             }
+            // the rest of the group: this session's next queued requests, in order
+            grp.push_back(r);
+            int64_t n_ins = (int64_t)r->ins_src.size(), n_del = (int64_t)r->del_src.size();
+            grp_bytes = r->est_bytes;
+            if (sv->coalesce > 1) {
+                for (auto it = sv->queue.begin(); it != sv->queue.end() && (int32_t)grp.size() < sv->coalesce;) {
+                    ServerRequest* c = sv->reqs[*it].get();
+                    if (c->session != r->session) { ++it; continue; }
+                    int64_t ni = n_ins + (int64_t)c->ins_src.size(), nd = n_del + (int64_t)c->del_src.size();
+                    int64_t bytes = update_bytes(ses->g->n, ses->g->m, ni, nd);
+                    if (ni + nd > sv->coalesce_edges || sv->in_use + bytes > sv->budget) break;
+                    grp.push_back(c);
+                    n_ins = ni; n_del = nd; grp_bytes = bytes;
+                    it = sv->queue.erase(it);
+                }
+            }
             ses->busy = true;
-            sv->in_use += r->est_bytes;
+            sv->in_use += grp_bytes;
             sv->inflight++;
             sv->max_inflight = std::max(sv->max_inflight, sv->inflight);
-            r->t_start = now_ms();
+            double t0 = now_ms();
+            for (auto* c : grp) c->t_start = t0;
         }
-        int rc = scc_update_batch(ses->g, ses->s, (int64_t)r->ins_src.size(), r->ins_src.data(), r->ins_dst.data(),
-                                  (int64_t)r->del_src.size(), r->del_src.data(), r->del_dst.data(), 0, &r->st);
+        int rc;
+        scc_update_stats st;
+        memset(&st, 0, sizeof(st));
+        if (grp.size() == 1) {
+            rc = scc_update_batch(ses->g, ses->s, (int64_t)r->ins_src.size(), r->ins_src.data(), r->ins_dst.data(),
+                                  (int64_t)r->del_src.size(), r->del_src.data(), r->del_dst.data(), 0, &st);
+        } else {
+            std::vector<int32_t> is, id, ds, dd;
+            compose_group(grp, is, id, ds, dd);
+            rc = scc_update_batch(ses->g, ses->s, (int64_t)is.size(), is.data(), id.data(), (int64_t)ds.size(),
+                                  ds.data(), dd.data(), 0, &st);
+        }
         {
             std::lock_guard<std::mutex> lk(sv->mu);
-            r->rc = rc;
-            r->t_done = now_ms();
-            r->done = true;
+            double t1 = now_ms();
             ses->busy = false;
-            sv->in_use -= r->est_bytes;
+            sv->in_use -= grp_bytes;
             sv->in_use -= ses->resident;
             ses->resident = graph_bytes(ses->g->n, ses->g->m) + state_bytes(ses->g->n);
             sv->in_use += ses->resident;
             sv->inflight--;
-            sv->completed++;
-            if (rc == SCC_OK) {
-                sv->latencies.push_back(r->t_done - r->t_submit);
-                sv->updates_done += (int64_t)(r->ins_src.size() + r->del_src.size());
+            sv->groups++;
+            for (auto* c : grp) {
+                c->rc = rc;
+                c->st = st;
+                c->t_done = t1;
+                c->done = true;
+                sv->completed++;
+                if (rc == SCC_OK) {
+                    sv->latencies.push_back(c->t_done - c->t_submit);
+                    sv->updates_done += (int64_t)(c->ins_src.size() + c->del_src.size());
+                }
+                c->ins_src.clear(); c->ins_src.shrink_to_fit(); c->ins_dst.clear(); c->ins_dst.shrink_to_fit();
+                c->del_src.clear(); c->del_src.shrink_to_fit(); c->del_dst.clear(); c->del_dst.shrink_to_fit();
             }
-            sv->t_last = std::max(sv->t_last, r->t_done);
-            r->ins_src.clear(); r->ins_src.shrink_to_fit(); r->ins_dst.clear(); r->ins_dst.shrink_to_fit();
-            r->del_src.clear(); r->del_src.shrink_to_fit(); r->del_dst.clear(); r->del_dst.shrink_to_fit();
+            sv->t_last = std::max(sv->t_last, t1);
         }
         sv->cv_done.notify_all();
         sv->cv_work.notify_all();
     }
+}
+
+extern "C" int scc_server_set_coalesce(scc_server* sv, int32_t max_requests, int64_t max_edges) {
+    SCC_REQUIRE(sv && max_requests >= 1 && max_edges >= 0, SCC_ERR_INVALID, "bad argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->coalesce = max_requests;
+    sv->coalesce_edges = max_edges;
+    return SCC_OK;
 }
 
 extern "C" int scc_server_create(int device, int num_slots, int64_t hbm_budget_bytes, scc_server** out) {
@@ -245,6 +360,7 @@ extern "C" int scc_server_get_stats(scc_server* sv, scc_server_stats* out) {
     out->updates_per_s = span > 0 ? sv->updates_done / (span * 1e-3) : 0.0;
     out->max_inflight = sv->max_inflight;
     out->bytes_in_use = sv->in_use;
+    out->groups = sv->groups;
     return SCC_OK;
 }
 

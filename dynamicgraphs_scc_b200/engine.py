@@ -537,6 +537,10 @@ class Server:
     def drain(self) -> None:
         call("scc_server_drain", self._h)
 
+    def set_coalesce(self, max_requests: int, max_edges: int = 1 << 24) -> None:
+        """Compose up to max_requests queued batches of a session into one update (1 = off)."""
+        call("scc_server_set_coalesce", self._h, int(max_requests), int(max_edges))
+
     def stats(self) -> dict:
         s = capi.ServerStats()
         call("scc_server_get_stats", self._h, C.byref(s))

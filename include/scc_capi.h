@@ -328,6 +328,7 @@ typedef struct scc_request_result {
 typedef struct scc_server_stats {
     int64_t completed, rejected, updates, max_inflight, bytes_in_use;
     double p50_ms, p99_ms, max_ms, updates_per_s;
+    int64_t groups;             /* device updates applied (fewer than completed when requests coalesce) */
 } scc_server_stats;
 
 /* num_slots worker threads; admission keeps resident graphs + admitted batches
@@ -339,6 +340,12 @@ int scc_server_add_graph(scc_server* sv, scc_graph* g, int32_t* session);
 /* Copies the batch (host arrays) and queues it; returns at once. */
 int scc_server_submit(scc_server* sv, int32_t session, int64_t n_ins, const int32_t* ins_src, const int32_t* ins_dst,
                       int64_t n_del, const int32_t* del_src, const int32_t* del_dst, int64_t* request_id);
+/* Coalescing, off by default (max_requests = 1): a session's queued requests,
+ * up to max_requests and max_edges edges in all, are composed into one batch
+ * with the same final graph as applying them in order (an insert survives
+ * unless a later request of the group deletes that pair) and applied by one
+ * update.  Each request of a group then reports the group's result. */
+int scc_server_set_coalesce(scc_server* sv, int32_t max_requests, int64_t max_edges);
 int scc_server_wait(scc_server* sv, int64_t request_id, scc_request_result* out);
 int scc_server_drain(scc_server* sv);
 int scc_server_get_stats(scc_server* sv, scc_server_stats* out);

@@ -92,3 +92,51 @@ def test_admission_by_hbm_budget(gpu):
     with pytest.raises(Exception):
         sv.add_graph(Graph.generate(rmat_scale=16, edge_factor=8, seed=1))   # larger than the budget left
     sv.free()
+
+
+def test_coalesced_requests_equal_sequential(gpu):
+    """With coalescing on, a session's queued batches are applied as one composed
+    batch; the final labels equal the sequential run's and Tarjan's, and the last
+    request of each session reports the same SCC count.  The batches insert and
+    later delete the same pairs, so the composition rule is exercised."""
+    n, s, d, _ = seeded_graph(rmat_scale=11, edge_factor=6, seed=9)
+    rng = np.random.default_rng(5)
+    batches = []
+    prev = None
+    for j in range(12):
+        ki, kd = int(rng.integers(20, 300)), int(rng.integers(10, 150))
+        pick = rng.integers(0, len(s), kd)
+        ins = (rng.integers(0, n, ki).astype(np.int32), rng.integers(0, n, ki).astype(np.int32))
+        dels = [s[pick].astype(np.int32), d[pick].astype(np.int32)]
+        if prev is not None:           # delete some pairs the previous batch inserted
+            dels[0] = np.concatenate([dels[0], prev[0][:10]]); dels[1] = np.concatenate([dels[1], prev[1][:10]])
+        batches.append((ins[0], ins[1], dels[0], dels[1]))
+        prev = ins
+
+    def serve(coalesce):
+        sv = Server(num_slots=2, hbm_budget_bytes=8 << 30)
+        if coalesce:
+            sv.set_coalesce(8)
+        sid = sv.add_graph(Graph.from_edges(n, s, d))
+        # hold the session busy with a first request so the rest queue up together
+        rids = [sv.submit(sid, *b) for b in batches]
+        res = [sv.wait(r) for r in rids]
+        sv.drain()
+        lab = sv.labels(sid)
+        st = sv.stats()
+        sv.free()
+        return res, lab, st
+
+    r_seq, l_seq, st_seq = serve(False)
+    r_co, l_co, st_co = serve(True)
+    assert all(r["status"] == 0 for r in r_seq + r_co)
+    assert np.array_equal(l_seq, l_co)
+    assert r_seq[-1]["num_sccs"] == r_co[-1]["num_sccs"]
+    assert st_seq["groups"] == len(batches)
+    assert st_co["groups"] < len(batches)          # some requests were composed
+    assert st_co["completed"] == len(batches)
+    ss, dd = s, d
+    for b in batches:
+        ss, dd = apply_batch(ss, dd, *b)
+    csr = O.build_csr(n, ss, dd)
+    assert np.array_equal(l_co, O.tarjan_canonical(csr[0], csr[1]))
