@@ -189,7 +189,7 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
 // components (so independent pieces get their own pivot), then one FW-BW
 // round over all classes at once.  Every class loses at least its pivot's SCC
 // per round, so the loop ends.
-int scc_impl_resolve_all(const scc_graph* g, scc_state* s) {
+int scc_impl_resolve_all(const scc_graph* g, scc_state* s, bool classes_split) {
     if (s->live_count < 0) SCC_TRY(scc_impl_compact_live(g, s, true));
     for (int round = 0; round < (1 << 30); ++round) {
         int32_t t = 0;
@@ -197,7 +197,8 @@ int scc_impl_resolve_all(const scc_graph* g, scc_state* s) {
         SCC_TRY(scc_impl_compact_live(g, s, false));
         if (s->live_count == 0) break;
         int32_t classes = 0;
-        SCC_TRY(scc_impl_uf_split(g, s, &classes));
+        if (round == 0 && classes_split && t == 0) classes = -1;   // nothing changed since the caller's split
+        else SCC_TRY(scc_impl_uf_split(g, s, &classes));
         int32_t live_before = s->live_count;
         int32_t found = 0, act = 0;
         SCC_TRY(scc_impl_fb_round(g, s, INT32_MIN, -1, &found, &act));

@@ -173,7 +173,8 @@ int scc_impl_wcc(const scc_graph* g, scc_state* s);
 int scc_impl_uf_split(const scc_graph* g, scc_state* s, int32_t* num_classes);
 bool scc_trace_on();
 void scc_impl_pivot_release(scc_state* s);   // frees the learned-pivot and logging buffers
-int scc_impl_resolve_all(const scc_graph* g, scc_state* s);
+// classes_split: the live classes are already weak components (a split ran last)
+int scc_impl_resolve_all(const scc_graph* g, scc_state* s, bool classes_split = false);
 int scc_impl_get_live_host(scc_state* s, std::vector<int32_t>& out);
 int scc_impl_count_colour(scc_state* s, int32_t color, int32_t* count);
 int scc_impl_build_graph_from_device_edges(int32_t n, int64_t m, const int32_t* d_src,

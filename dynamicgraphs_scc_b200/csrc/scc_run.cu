@@ -117,7 +117,7 @@ static int run_method(const scc_graph* g, scc_state* s, int method, scc_run_stat
     }
     SCC_TRY(record(s, 4));
     // FB: start_workers_fw_bw_dfs
-    if (s->live_count > 0) SCC_TRY(scc_impl_resolve_all(g, s));
+    if (s->live_count > 0) SCC_TRY(scc_impl_resolve_all(g, s, method == SCC_METHOD_GLOBAL_WCC_FB));
     SCC_TRY(record(s, 5));
     return SCC_OK;
 }
