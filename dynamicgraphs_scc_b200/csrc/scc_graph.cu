@@ -84,6 +84,15 @@ __global__ void k_fill_offsets(int64_t m, int32_t n, const unsigned long long* _
     }
 }
 
+// begin[v] = first index i with keys[i] >= v, for v in [0, n]; 32-bit keys sorted.
+__global__ void k_fill_offsets32(int64_t m, int32_t n, const int32_t* __restrict__ keys, int32_t* __restrict__ begin) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= m; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t prev = (i == 0) ? -1 : (int64_t)keys[i - 1];
+        int64_t cur = (i == m) ? (int64_t)n : (int64_t)keys[i];
+        for (int64_t v = prev + 1; v <= cur && v <= n; ++v) begin[v] = (int32_t)i;
+    }
+}
+
 __global__ void k_low_words(int64_t m, const unsigned long long* __restrict__ keys, int32_t* __restrict__ out) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
         out[i] = (int32_t)(uint32_t)(keys[i] & 0xFFFFFFFFull);
@@ -205,15 +214,49 @@ int scc_impl_build_graph_from_device_edges(int32_t n, int64_t m, const int32_t* 
     return SCC_OK;
 }
 
-int scc_impl_transpose(scc_graph* g, cudaStream_t st) {
-    int32_t* src = nullptr;
-    SCC_CUDA(cudaMalloc(&src, sizeof(int32_t) * (size_t)(g->m > 0 ? g->m : 1)));
-    k_expand_sources<<<scc_blocks((int64_t)g->n * 32, 256, 148 * 64), 256, 0, st>>>(g->n, g->begin, src);
+// Stream-ordered scratch, released on the same stream.
+struct AsyncScratch {
+    void* p = nullptr;
+    cudaStream_t st;
+    explicit AsyncScratch(cudaStream_t s) : st(s) {}
+    ~AsyncScratch() { if (p) cudaFreeAsync(p, st); }
+    cudaError_t alloc(size_t bytes) { return cudaMallocAsync(&p, bytes > 0 ? bytes : 16, st); }
+};
+
+// Transpose of g's forward CSR into g->r_begin / g->r_node_idx (allocated):
+// a stable radix sort of (destination, source) pairs taken in edge order, so
+// every in-list comes out sorted by source -- gm_graph's make_reverse_edges
+// order (gm_graph/src/gm_graph.cc:193-287), duplicates kept.
+static int transpose_into(scc_graph* g, cudaStream_t st) {
+    const int64_t m = g->m;
+    const int32_t n = g->n;
+    if (m == 0) {
+        SCC_CUDA(cudaMemsetAsync(g->r_begin, 0, sizeof(int32_t) * ((size_t)n + 1), st));
+        return SCC_OK;
+    }
+    AsyncScratch src(st), keys(st), tmp(st);
+    SCC_CUDA(src.alloc(sizeof(int32_t) * (size_t)m));
+    SCC_CUDA(keys.alloc(sizeof(int32_t) * (size_t)m));
+    k_expand_sources<<<scc_blocks((int64_t)n * 32, 256, 148 * 64), 256, 0, st>>>(n, g->begin, (int32_t*)src.p);
     SCC_CUDA(cudaPeekAtLastError());
-    int64_t m2 = 0;
-    int s = build_side(g->n, g->m, g->node_idx, src, SCC_BUILD_KEEP_ALL, st, &g->r_begin, &g->r_node_idx, &m2);
-    cudaFree(src);
-    return s;
+    size_t tb = 0;
+    SCC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, g->node_idx, (int32_t*)keys.p, (const int32_t*)src.p,
+                                             g->r_node_idx, (int)m, 0, bits_for(n), st));
+    SCC_CUDA(tmp.alloc(tb));
+    SCC_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, g->node_idx, (int32_t*)keys.p, (const int32_t*)src.p,
+                                             g->r_node_idx, (int)m, 0, bits_for(n), st));
+    k_fill_offsets32<<<scc_blocks(m + 1, 256, 148 * 64), 256, 0, st>>>(m, n, (const int32_t*)keys.p, g->r_begin);
+    SCC_CUDA(cudaPeekAtLastError());
+    return SCC_OK;
+}
+
+int scc_impl_transpose(scc_graph* g, cudaStream_t st) {
+    size_t nb = sizeof(int32_t) * ((size_t)g->n + 1), mb = sizeof(int32_t) * (size_t)(g->m > 0 ? g->m : 1);
+    SCC_CUDA(cudaMalloc(&g->r_begin, nb));
+    SCC_CUDA(cudaMalloc(&g->r_node_idx, mb));
+    SCC_TRY(transpose_into(g, st));
+    SCC_CUDA(cudaStreamSynchronize(st));
+    return SCC_OK;
 }
 
 // ------------------------------------------------------------------ C ABI
@@ -303,6 +346,17 @@ extern "C" int scc_graph_upload_csr(scc_graph* g, const int32_t* begin, const in
         SCC_CUDA(cudaMemcpyAsync(g->r_node_idx, r_node_idx, mb, cudaMemcpyHostToDevice, st));
     }
     return SCC_OK;
+}
+
+extern "C" int scc_graph_upload_csr_out(scc_graph* g, const int32_t* begin, const int32_t* node_idx, void* stream) {
+    SCC_REQUIRE(g && begin && (g->m == 0 || node_idx), SCC_ERR_INVALID, "NULL argument");
+    SCC_CUDA(cudaSetDevice(g->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    g->self_loops = -1;                      // new contents: count again when needed
+    SCC_CUDA(cudaMemcpyAsync(g->begin, begin, sizeof(int32_t) * ((size_t)g->n + 1), cudaMemcpyHostToDevice, st));
+    if (g->m > 0)
+        SCC_CUDA(cudaMemcpyAsync(g->node_idx, node_idx, sizeof(int32_t) * (size_t)g->m, cudaMemcpyHostToDevice, st));
+    return transpose_into(g, st);
 }
 
 extern "C" int scc_graph_free(scc_graph* g) {

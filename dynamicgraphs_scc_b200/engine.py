@@ -113,6 +113,17 @@ class Graph:
         call("scc_graph_copy_csr", self.handle, i32p(b), i32p(a), i32p(rb), i32p(ra))
         return b, a, rb, ra
 
+    def upload_csr(self, begin, node_idx, r_begin=None, r_node_idx=None, stream: int = 0) -> None:
+        """Replace the graph's contents with host CSR arrays of the same n and m; without a
+        transpose, only the forward CSR crosses the bus and the transpose is rebuilt on the device."""
+        b, a = _i32(begin), _i32(node_idx)
+        if r_begin is None:
+            call("scc_graph_upload_csr_out", self.handle, b.ctypes.data, a.ctypes.data, stream or None)
+        else:
+            rb, ra = _i32(r_begin), _i32(r_node_idx)
+            call("scc_graph_upload_csr", self.handle, b.ctypes.data, a.ctypes.data, rb.ctypes.data, ra.ctypes.data,
+                 stream or None)
+
     def save_binary(self, path: str) -> None:
         call("scc_graph_save_binary", self.handle, path.encode())
 
