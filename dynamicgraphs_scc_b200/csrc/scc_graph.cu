@@ -12,6 +12,7 @@
 #include <stdarg.h>
 #include <stdlib.h>
 #include <string.h>
+#include <mutex>
 #include "scc_internal.cuh"
 
 // ------------------------------------------------------------------ errors
@@ -220,7 +221,7 @@ struct AsyncScratch {
     cudaStream_t st;
     explicit AsyncScratch(cudaStream_t s) : st(s) {}
     ~AsyncScratch() { if (p) cudaFreeAsync(p, st); }
-    cudaError_t alloc(size_t bytes) { return cudaMallocAsync(&p, bytes > 0 ? bytes : 16, st); }
+    cudaError_t alloc(size_t bytes) { return scc_impl_malloc_async(&p, bytes > 0 ? bytes : 16, st); }
 };
 
 // Transpose of g's forward CSR into g->r_begin / g->r_node_idx (allocated):
@@ -479,4 +480,52 @@ extern "C" int scc_graph_load_edge_list(const char* path, int device, scc_graph*
     }
     return scc_graph_create_edges((int32_t)maxid, (int64_t)src.size(), src.data(), dst.data(), SCC_BUILD_KEEP_ALL,
                                   device, out);
+}
+
+// ------------------------------------------------------------------ memory pool
+// One pool per device, owned by the library (the device's default pool and
+// other libraries' pools are left alone).  Its release threshold keeps freed
+// blocks reserved, so repeated uploads and updates reuse them.
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pools[64] = {};
+
+static cudaError_t pool_of(int device, cudaMemPool_t* out) {
+    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[device]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaError_t e = cudaMemPoolCreate(&g_pools[device], &props);
+        if (e != cudaSuccess) { g_pools[device] = nullptr; return e; }
+        uint64_t keep = UINT64_MAX;
+        e = cudaMemPoolSetAttribute(g_pools[device], cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+    }
+    *out = g_pools[device];
+    return cudaSuccess;
+}
+
+cudaError_t scc_impl_malloc_async(void** p, size_t bytes, cudaStream_t st) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    cudaMemPool_t pool = nullptr;
+    if (e == cudaSuccess) e = pool_of(device, &pool);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+    return e;
+}
+
+extern "C" int scc_release_cached_memory(int device) {
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        if (device < 0 || device >= 64 || !g_pools[device]) return SCC_OK;
+        pool = g_pools[device];
+    }
+    SCC_CUDA(cudaSetDevice(device));
+    SCC_CUDA(cudaDeviceSynchronize());
+    SCC_CUDA(cudaMemPoolTrimTo(pool, 0));
+    return SCC_OK;
 }

@@ -172,6 +172,10 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
 int scc_impl_wcc(const scc_graph* g, scc_state* s);
 int scc_impl_uf_split(const scc_graph* g, scc_state* s, int32_t* num_classes);
 bool scc_trace_on();
+// Stream-ordered scratch from the library's own memory pool on the current
+// device: freed blocks stay reserved for the next call (no re-mapping of
+// gigabytes per upload or update) until scc_release_cached_memory.
+cudaError_t scc_impl_malloc_async(void** p, size_t bytes, cudaStream_t st);
 void scc_impl_pivot_release(scc_state* s);   // frees the learned-pivot and logging buffers
 // classes_split: the live classes are already weak components (a split ran last)
 int scc_impl_resolve_all(const scc_graph* g, scc_state* s, bool classes_split = false);

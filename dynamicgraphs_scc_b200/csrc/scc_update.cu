@@ -200,7 +200,7 @@ struct DevBuf {
 
 static int alloc(DevBuf& b, size_t bytes, cudaStream_t st) {
     b.st = st;
-    SCC_CUDA(cudaMallocAsync(&b.p, bytes > 0 ? bytes : 16, st));
+    SCC_CUDA(scc_impl_malloc_async(&b.p, bytes > 0 ? bytes : 16, st));
     return SCC_OK;
 }
 
@@ -256,7 +256,7 @@ static int merge_side(int32_t n, int64_t m, const int32_t* off, const int32_t* a
         SCC_CUDA(cudaPeekAtLastError());
     }
     int32_t* noff = nullptr;
-    SCC_CUDA(cudaMallocAsync(&noff, sizeof(int32_t) * ((size_t)n + 1), st));
+    SCC_CUDA(scc_impl_malloc_async((void**)&noff, sizeof(int32_t) * ((size_t)n + 1), st));
     size_t bytes = 0;
     SCC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, deg.as<int32_t>(), noff, n + 1, st));
     SCC_TRY(alloc(tmp, bytes, st));
@@ -265,8 +265,8 @@ static int merge_side(int32_t n, int64_t m, const int32_t* off, const int32_t* a
     SCC_CUDA(cudaMemcpyAsync(&nm, noff + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     SCC_CUDA(cudaStreamSynchronize(st));
     int32_t* nadj = nullptr;
-    cudaError_t e = cudaMallocAsync(&nadj, sizeof(int32_t) * (size_t)(nm > 0 ? nm : 1), st);
-    if (e != cudaSuccess) { cudaFreeAsync(noff, st); return scc_cuda_status(e, "cudaMallocAsync", __FILE__, __LINE__); }
+    cudaError_t e = scc_impl_malloc_async((void**)&nadj, sizeof(int32_t) * (size_t)(nm > 0 ? nm : 1), st);
+    if (e != cudaSuccess) { cudaFreeAsync(noff, st); return scc_cuda_status(e, "scratch allocation", __FILE__, __LINE__); }
     if (n > 0) {
         k_upd_merge<<<scc_blocks((int64_t)n * 32, SCC_THREADS, 148 * 16), SCC_THREADS, 0, st>>>(
             n, off, adj, dead.as<uint8_t>(), ndead.as<int32_t>(), ins, insb.as<int32_t>(), noff, nadj,

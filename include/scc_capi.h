@@ -57,6 +57,10 @@ const char* scc_status_string(int status);
 const char* scc_last_error(void);
 int scc_version(void);                       /* major*10000 + minor*100 + patch */
 int scc_device_count(int* count);
+/* Scratch of uploads, updates and graph merges comes from one memory pool per
+ * device owned by this library, which keeps freed blocks for reuse; this hands
+ * them back to the driver (after synchronising the device). */
+int scc_release_cached_memory(int device);
 
 /* ---- graph (gm_graph / GPUGraph) ---------------------------------------------------- */
 /* Build flags for scc_graph_create_edges*. */
