@@ -392,6 +392,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     torch.cuda.set_device(local_rank)
     from dynamicgraphs_scc_b200 import Graph, State, capi
+    from dynamicgraphs_scc_b200.replicas import reduce_replicas
 
     kw = WORKLOADS[args.workload]
     learned = args.workload == "c3"            # the learned-pivot configuration
@@ -439,11 +440,7 @@ def main():
         capi.call("scc_state_profile_read", st.handle, C.byref(l_ms), C.byref(l_launch), C.byref(l_items),
                   C.byref(l_edges))
         capi.call("scc_state_profile", st.handle, 0)
-        ms = ev0.elapsed_time(ev1) / args.steps
-        if dist is not None:
-            t = torch.tensor([ms], device=f"cuda:{local_rank}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms, _ = reduce_replicas(ev0.elapsed_time(ev1) / args.steps, m, dist, f"cuda:{local_rank}")
         return ms, kernels, phase, clocks, (l_ms, l_launch, l_items, l_edges)
 
     plain = None
@@ -456,7 +453,7 @@ def main():
     l_ms, l_launch, l_items, l_edges = ledger
     if learned and rank == 0:
         plain["labels_equal_learned"] = bool(np.array_equal(plain_labels, st.canonical_labels()))
-    total_edges = m * world
+    _, total_edges = reduce_replicas(ms, m, dist, f"cuda:{local_rank}")
     gteps = total_edges / (ms * 1e-3) / 1e9
 
     # roofline of the whole step (algorithmic bytes 16M + 20N + 8)
@@ -499,10 +496,7 @@ def main():
         if i > 0:
             e2e_ms.append(e0.elapsed_time(e1))
     e2e = statistics.mean(e2e_ms) if e2e_ms else float("nan")
-    if dist is not None:
-        t = torch.tensor([e2e], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = float(t.item())
+    e2e, _ = reduce_replicas(e2e, m, dist, f"cuda:{local_rank}")
     e2e_gteps = total_edges / (e2e * 1e-3) / 1e9 if e2e_ms else None
     h2d = 4 * ((n + 1) + m)
     d2h = 4 * n
