@@ -174,6 +174,7 @@ _SIGS = {
     "scc_server_set_coalesce": [_P, C.c_int32, C.c_int64],
     "scc_graph_upload_csr_out": [_P, _P, _P, _P],
     "scc_release_cached_memory": [C.c_int],
+    "scc_debug_inject": [C.c_int, C.c_int64],
     "scc_server_wait": [_P, C.c_int64, C.POINTER(RequestResult)],
     "scc_server_drain": [_P],
     "scc_server_get_stats": [_P, C.POINTER(ServerStats)],

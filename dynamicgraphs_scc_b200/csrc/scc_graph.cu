@@ -12,6 +12,7 @@
 #include <stdarg.h>
 #include <stdlib.h>
 #include <string.h>
+#include <atomic>
 #include <mutex>
 #include "scc_internal.cuh"
 
@@ -508,7 +509,25 @@ static cudaError_t pool_of(int device, cudaMemPool_t* out) {
     return cudaSuccess;
 }
 
+// Host-side fault injection (scc_debug_inject): the n-th pool allocation from
+// now fails; the next asynchronous drain gets one queue slot nobody fills.
+static std::atomic<int64_t> g_fail_alloc_in{0};
+static std::atomic<int> g_wait_hole{0};
+
+extern "C" int scc_debug_inject(int what, int64_t countdown) {
+    SCC_REQUIRE(countdown >= 0, SCC_ERR_INVALID, "countdown %lld", (long long)countdown);
+    if (what == SCC_INJECT_ALLOC) { g_fail_alloc_in = countdown; return SCC_OK; }
+    if (what == SCC_INJECT_WAIT) { g_wait_hole = countdown > 0 ? 1 : 0; return SCC_OK; }
+    scc_set_error("unknown injection %d", what);
+    return SCC_ERR_INVALID;
+}
+
+bool scc_impl_take_wait_injection() { return g_wait_hole.exchange(0) != 0; }
+
 cudaError_t scc_impl_malloc_async(void** p, size_t bytes, cudaStream_t st) {
+    int64_t k = g_fail_alloc_in.load();
+    while (k > 0 && !g_fail_alloc_in.compare_exchange_weak(k, k - 1)) {}
+    if (k == 1) { *p = nullptr; return cudaErrorMemoryAllocation; }
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     cudaMemPool_t pool = nullptr;

@@ -176,6 +176,7 @@ bool scc_trace_on();
 // device: freed blocks stay reserved for the next call (no re-mapping of
 // gigabytes per upload or update) until scc_release_cached_memory.
 cudaError_t scc_impl_malloc_async(void** p, size_t bytes, cudaStream_t st);
+bool scc_impl_take_wait_injection();   // consumes a pending SCC_INJECT_WAIT
 void scc_impl_pivot_release(scc_state* s);   // frees the learned-pivot and logging buffers
 // classes_split: the live classes are already weak components (a split ran last)
 int scc_impl_resolve_all(const scc_graph* g, scc_state* s, bool classes_split = false);

@@ -559,6 +559,13 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
             int32_t init[CTR_AWORK - CTR_AHEAD + 1] = {0};   // head, tail, work on separate lines
             init[CTR_ATAIL - CTR_AHEAD] = qlen;
             init[CTR_AWORK - CTR_AHEAD] = qlen;
+            if (scc_impl_take_wait_injection()) {
+                // injected failure: one more item is announced than written, so
+                // the warp that takes slot qlen (kept at -1) waits until its
+                // bound runs out and the drain reports SCC_ERR_TIMEOUT
+                init[CTR_ATAIL - CTR_AHEAD] = qlen + 1;
+                init[CTR_AWORK - CTR_AHEAD] = qlen + 1;
+            }
             SCC_CUDA(cudaMemcpyAsync(s->ctr + CTR_AHEAD, init, sizeof(init), cudaMemcpyHostToDevice, s->stream));
             SCC_TRY(scc_zero_counters(s, CTR_ASYNC_ITEMS, 4));
             SCC_TRY(scc_zero_counters(s, CTR_ABAIL, 1));

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <map>
 #include <string.h>
+#include <nvtx3/nvToolsExt.h>
 #include "scc_internal.cuh"
 
 // ------------------------------------------------------------------ kernels
@@ -58,8 +59,15 @@ static int canonical_into(scc_state* s, int32_t* d_out) {
     return SCC_OK;
 }
 
+// Phase markers: a CUDA event on the state's stream (the run statistics) and
+// an NVTX range per phase for profilers, named like the reference's -d output.
+static const char* const kPhase[5] = {"TRIM1", "GLOBAL_FW_BW", "TRIM1_TRIM2", "WCC", "FW_BW"};
+static thread_local int t_nvtx_open = 0;
+
 static int record(scc_state* s, int i) {
     SCC_CUDA(cudaEventRecord(s->ev[i], s->stream));
+    if (t_nvtx_open) { nvtxRangePop(); t_nvtx_open = 0; }
+    if (i < 5) { nvtxRangePushA(kPhase[i]); t_nvtx_open = 1; }
     return SCC_OK;
 }
 static double elapsed(scc_state* s, int a, int b) {
@@ -143,7 +151,10 @@ extern "C" int scc_run(const scc_graph* g, scc_state* s, int method, int pivot_m
     if (pivot_mode == SCC_PIVOT_LEARNED)
         SCC_REQUIRE(s->pivot_model, SCC_ERR_INVALID, "learned pivots need a model (scc_state_set_pivot_model)");
     s->pivot_mode = pivot_mode;
+    nvtxRangePushA("scc_run");
     int rc = run_method(g, s, method, &st);
+    if (t_nvtx_open) { nvtxRangePop(); t_nvtx_open = 0; }
+    nvtxRangePop();
     s->pivot_mode = SCC_PIVOT_DEGREE;
     if (rc != SCC_OK) return rc;
     SCC_CUDA(cudaStreamSynchronize(s->stream));

@@ -61,6 +61,17 @@ int scc_device_count(int* count);
  * device owned by this library, which keeps freed blocks for reuse; this hands
  * them back to the driver (after synchronising the device). */
 int scc_release_cached_memory(int device);
+/* Host-side fault injection for failure-path tests (the reference's only
+ * failure path is CUDA_CHECK -> exit(1), src_CUDA/scc_cuda.h:61-67).
+ * SCC_INJECT_ALLOC: the countdown-th scratch allocation of an upload or update
+ * from now fails (SCC_ERR_OOM); 0 disarms.  SCC_INJECT_WAIT (countdown > 0):
+ * the next asynchronous reachability drain is given one queue slot that is
+ * never filled, so its bounded wait gives up and the call returns
+ * SCC_ERR_TIMEOUT; the state is usable again after scc_state_reset.  No
+ * injection faults, traps or hangs the GPU. */
+#define SCC_INJECT_ALLOC 1
+#define SCC_INJECT_WAIT  2
+int scc_debug_inject(int what, int64_t countdown);
 
 /* ---- graph (gm_graph / GPUGraph) ---------------------------------------------------- */
 /* Build flags for scc_graph_create_edges*. */
