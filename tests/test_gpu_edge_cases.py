@@ -1,0 +1,77 @@
+"""GPU: structural edge cases, each compared with the oracle's Tarjan for the
+three methods.  Each case exercises one path: the deepest peel cascades
+(a long path), the asynchronous drain on a long chain of hops (a long cycle),
+edge-parallel hub expansion (a bidirectional star above the hub threshold),
+warp-cooperative lists (a clique), self-loops that must not keep a vertex
+alive, many tiny classes (thousands of disjoint 3-cycles), and one giant SCC
+of long diameter (a fully bidirectional grid)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from dynamicgraphs_scc_b200 import Graph, State
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(n, s, d):
+    s = np.asarray(s, np.int32); d = np.asarray(d, np.int32)
+    csr = O.build_csr(n, s, d)
+    exp = O.tarjan_canonical(csr[0], csr[1])
+    g = Graph.from_edges(n, s, d)
+    st = State(g)
+    for method in (0, 1, 2):
+        st.reset()
+        r = st.run(method)
+        assert np.array_equal(st.canonical_labels(), exp), method
+        assert r["num_sccs"] == len(np.unique(exp)), method
+    st.free(); g.free()
+
+
+def test_long_path_all_trimmed(gpu):
+    n = 300000
+    s = np.arange(n - 1); _check(n, s, s + 1)
+
+
+def test_long_cycle(gpu):
+    n = 200000
+    s = np.arange(n); _check(n, s, (s + 1) % n)
+
+
+def test_bidirectional_star_with_huge_hub(gpu):
+    leaves = 20000                                   # hub degree far above the 4,096 hub threshold
+    l = np.arange(1, leaves + 1)
+    _check(leaves + 1, np.concatenate([np.zeros(leaves, int), l]), np.concatenate([l, np.zeros(leaves, int)]))
+
+
+def test_clique(gpu):
+    k = 300
+    a, b = np.meshgrid(np.arange(k), np.arange(k), indexing="ij")
+    keep = a != b
+    _check(k, a[keep], b[keep])
+
+
+def test_self_loops_only(gpu):
+    n = 10000
+    s = np.arange(n); _check(n, s, s)
+
+
+def test_many_disjoint_triangles(gpu):
+    t = 5000
+    base = np.arange(t) * 3
+    s = np.concatenate([base, base + 1, base + 2]); d = np.concatenate([base + 1, base + 2, base])
+    _check(3 * t, s, d)
+
+
+def test_fully_bidirectional_grid(gpu):
+    side = 300
+    idx = np.arange(side * side).reshape(side, side)
+    h = (idx[:, :-1].ravel(), idx[:, 1:].ravel()); v = (idx[:-1, :].ravel(), idx[1:, :].ravel())
+    s = np.concatenate([h[0], h[1], v[0], v[1]]); d = np.concatenate([h[1], h[0], v[1], v[0]])
+    _check(side * side, s, d)
+
+
+def test_single_vertex_cases(gpu):
+    _check(1, [0], [0])                              # one vertex with a self-loop
+    _check(2, [0, 1], [1, 0])                        # a 2-cycle
+    _check(3, [0, 0, 0], [1, 1, 1])                  # duplicates only
