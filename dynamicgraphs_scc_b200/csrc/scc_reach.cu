@@ -591,6 +591,18 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
                 double t1 = now_ms();
                 fprintf(stderr, "[scc] reach async seeds=%d spilled=%d %.3f ms\n", qlen, s->h_ctr[CTR_ATAIL], t1 - t0);
             }
+            if (s->h_ctr[CTR_ERROR] == SCC_DEVERR_WAIT_LIMIT && s->h_ctr[CTR_ERROR_INFO] == 1 &&
+                (s->h_ctr[CTR_AWORK] == 0 || s->h_ctr[CTR_ABAIL])) {
+                // Idle warps gave up while a warp walked a long chain of single
+                // hops: the chain stays in that warp's own buffer, so the work
+                // count sits still for seconds and their idle bound cannot tell it
+                // from a stall.  Warps still busy drain the queue before they read
+                // the error word, so a drain that ended with no work outstanding,
+                // or that handed its frontier back, is complete.
+                if (scc_trace_on()) fprintf(stderr, "[scc] reach async: idle warps left a long chain early\n");
+                s->h_ctr[CTR_ERROR] = 0;
+                SCC_CUDA(cudaMemsetAsync(s->ctr + CTR_ERROR, 0, sizeof(int32_t) * 2, s->stream));
+            }
             if (s->h_ctr[CTR_ERROR]) {
                 // leave the queue clean for the next traversal, then report
                 SCC_CUDA(cudaMemsetAsync(s->aq, 0xFF, sizeof(int32_t) * (size_t)qcap, s->stream));

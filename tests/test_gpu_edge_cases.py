@@ -75,3 +75,17 @@ def test_single_vertex_cases(gpu):
     _check(1, [0], [0])                              # one vertex with a self-loop
     _check(2, [0, 1], [1, 0])                        # a 2-cycle
     _check(3, [0, 0, 0], [1, 1, 1])                  # duplicates only
+
+
+def test_very_long_cycle_completes(gpu):
+    # one SCC crossed by a single chain of 2,000,000 hops: the asynchronous
+    # drain runs for seconds with one item outstanding, and idle warps must
+    # keep waiting (their bound counts stalls, not traversal length)
+    n = 2000000
+    s = np.arange(n, dtype=np.int32)
+    g = Graph.from_edges(n, s, ((s + 1) % n).astype(np.int32))
+    st = State(g)
+    r = st.run(2)
+    assert r["num_sccs"] == 1 and r["first_scc_size"] == n
+    assert not st.canonical_labels().any()
+    st.free(); g.free()
