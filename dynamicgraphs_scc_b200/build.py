@@ -34,6 +34,7 @@ CU_SOURCES = [
     "scc_tune.cu",
     "scc_server.cu",
     "scc_mlp.cu",
+    "scc_levels.cu",
 ]
 
 

@@ -168,6 +168,10 @@ _SIGS = {
     "scc_decremental_delete": [_P, _P, C.c_int64, _I32P, _I32P, C.POINTER(UpdateStats)],
     "scc_insert_idea1": [_P, _P, C.c_int64, _I32P, _I32P, C.POINTER(RunStats)],
     "scc_condensation_graph": [_P, _I32P, C.c_int32, C.c_int64, _I32P, _I32P, C.POINTER(_P)],
+    "scc_topological_levels": [_P, _I32P, _I32P],
+    "scc_read_edge_list": [C.c_char_p, C.c_int64, _I32P, _I32P, C.POINTER(C.c_int64), _I32P],
+    "scc_affected_levels": [_P, _I32P, C.c_int32, C.c_int32, _I32P, C.c_int64, _I32P, _I32P, _I32P, _I32P],
+    "scc_state_finish_unaffected": [_P, _I32P, _I32P, C.c_int32, _I32P],
     "scc_server_create": [C.c_int, C.c_int, C.c_int64, C.POINTER(_P)],
     "scc_server_add_graph": [_P, _P, _I32P],
     "scc_server_submit": [_P, C.c_int32, C.c_int64, _I32P, _I32P, C.c_int64, _I32P, _I32P, _I64P],

@@ -443,10 +443,10 @@ extern "C" int scc_graph_load_binary(const char* path, int device, scc_graph** o
     return scc_graph_create_csr((int32_t)hdr[0], (int32_t)hdr[1], b.data(), a.data(), nullptr, nullptr, device, out);
 }
 
-// Fast text parser: "u v" per line, 1-based; N = max id (src/common_main.h:61-83,
+// Fast text parser: "u v" per line, 1-based, stored 0-based; returns the
+// largest id, the reference's N (src/common_main.h:61-83,
 // src_CUDA/scc_cuda_dynamic.cpp:59-147).
-extern "C" int scc_graph_load_edge_list(const char* path, int device, scc_graph** out) {
-    SCC_REQUIRE(path && out, SCC_ERR_INVALID, "NULL argument");
+static int parse_edge_list(const char* path, std::vector<int32_t>& src, std::vector<int32_t>& dst, int64_t* max_id) {
     FILE* f = fopen(path, "rb");
     SCC_REQUIRE(f, SCC_ERR_IO, "cannot open %s", path);
     fseek(f, 0, SEEK_END);
@@ -456,7 +456,6 @@ extern "C" int scc_graph_load_edge_list(const char* path, int device, scc_graph*
     size_t rd = sz > 0 ? fread(buf.data(), 1, (size_t)sz, f) : 0;
     fclose(f);
     buf[rd] = 0;
-    std::vector<int32_t> src, dst;
     int64_t maxid = 0;
     const char* p = buf.data();
     const char* end = p + rd;
@@ -479,8 +478,35 @@ extern "C" int scc_graph_load_edge_list(const char* path, int device, scc_graph*
         if (v[0] > maxid) maxid = v[0];
         if (v[1] > maxid) maxid = v[1];
     }
+    *max_id = maxid;
+    return SCC_OK;
+}
+
+extern "C" int scc_graph_load_edge_list(const char* path, int device, scc_graph** out) {
+    SCC_REQUIRE(path && out, SCC_ERR_INVALID, "NULL argument");
+    std::vector<int32_t> src, dst;
+    int64_t maxid = 0;
+    SCC_TRY(parse_edge_list(path, src, dst, &maxid));
     return scc_graph_create_edges((int32_t)maxid, (int64_t)src.size(), src.data(), dst.data(), SCC_BUILD_KEEP_ALL,
                                   device, out);
+}
+
+extern "C" int scc_read_edge_list(const char* path, int64_t capacity, int32_t* src, int32_t* dst, int64_t* count,
+                                  int32_t* max_id) {
+    SCC_REQUIRE(path && count && capacity >= 0, SCC_ERR_INVALID, "bad argument");
+    std::vector<int32_t> s, d;
+    int64_t maxid = 0;
+    SCC_TRY(parse_edge_list(path, s, d, &maxid));
+    *count = (int64_t)s.size();
+    if (max_id) *max_id = (int32_t)maxid;
+    if (capacity > 0) {
+        SCC_REQUIRE(src && dst, SCC_ERR_INVALID, "NULL output arrays");
+        SCC_REQUIRE(capacity >= (int64_t)s.size(), SCC_ERR_INVALID, "capacity %lld below %lld edges",
+                    (long long)capacity, (long long)s.size());
+        memcpy(src, s.data(), sizeof(int32_t) * s.size());
+        memcpy(dst, d.data(), sizeof(int32_t) * d.size());
+    }
+    return SCC_OK;
 }
 
 // ------------------------------------------------------------------ memory pool

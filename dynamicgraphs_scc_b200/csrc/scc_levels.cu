@@ -1,0 +1,319 @@
+// Method 7's level analytics on the condensation graph: topological levels of
+// the DAG (the BFS in create_scc_edges, src/common_main.h:85-108, 210-219),
+// the levels an inserted batch can affect (affect_level and its prefix sum,
+// :232-262), and the trim shortcut that finishes every node of an unaffected
+// level as its own SCC (src/scc_trim1.cc:67-73).
+//
+// The reference computes levels with a FIFO queue (Kahn's order): a node is
+// queued when its last predecessor is processed, and every processed edge
+// overwrites the child's level with the parent's level + 1.  The queue's
+// levels never decrease, so the last write is the largest, and a level is the
+// longest path from a source.  Here the peel runs without an order: released
+// nodes are expanded from per-warp queues in shared memory, each edge raises
+// its child's level with atomicMax before it decrements the child's
+// in-count, and whoever brings the count to zero releases the child.  Nodes
+// that are never released (on or behind a cycle, when the labels are not the
+// SCCs of the graph) keep the largest level + 1 of their released
+// predecessors, or 0 -- what the reference's queue leaves them.
+#include <cub/cub.cuh>
+#include "scc_internal.cuh"
+
+#define LEVEL_Q 256          // per-warp queue of released nodes awaiting expansion
+
+struct LevelArgs {
+    const int32_t* begin; const int32_t* node_idx; const int32_t* r_begin;
+    int32_t* cnt; int32_t* level; int32_t* ovf; int32_t* ovf_count;
+};
+
+__global__ void k_level_init(int32_t n, const int32_t* __restrict__ r_begin, int32_t* __restrict__ cnt,
+                             int32_t* __restrict__ level) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        cnt[i] = __ldg(r_begin + i + 1) - __ldg(r_begin + i);
+        level[i] = 0;
+    }
+}
+
+// Expand this warp's released nodes 32 at a time, their out-edges spread over
+// the lanes (warp prefix sum of the degrees, owner found by a binary search
+// over the lanes).  A released node's level is final: each of its
+// predecessors raised it before the fence that precedes their decrement.
+__device__ void level_drain(const LevelArgs& a, int32_t* wq, int32_t& qn) {
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xFFFFFFFFu;
+    while (qn > 0) {
+        const int32_t take = min(qn, 32);
+        qn -= take;
+        const int32_t x = lane < take ? wq[qn + lane] : -1;
+        __syncwarp();
+        __threadfence();
+        int32_t ob = 0, od = 0, lx = 0;
+        if (x >= 0) {
+            ob = __ldg(a.begin + x);
+            od = __ldg(a.begin + x + 1) - ob;
+            lx = __ldcg(a.level + x) + 1;
+        }
+        int32_t incl = od;
+        for (int o = 1; o < 32; o <<= 1) {
+            int32_t t = __shfl_up_sync(full, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int32_t total = __shfl_sync(full, incl, 31);
+        const int32_t excl = incl - od;
+        for (int32_t j0 = 0; j0 < total; j0 += 32) {
+            const int32_t j = j0 + lane;
+            int owner = 0;                                   // largest lane with excl <= j
+            for (int step = 16; step > 0; step >>= 1) {
+                int cand = owner + step;
+                int32_t ev = __shfl_sync(full, excl, cand);
+                if (ev <= j) owner = cand;
+            }
+            const int32_t k = j - __shfl_sync(full, excl, owner);
+            const int32_t oob = __shfl_sync(full, ob, owner);
+            const int32_t olx = __shfl_sync(full, lx, owner);
+            int32_t nv = -1;
+            if (j < total) {
+                int32_t w = __ldg(a.node_idx + oob + k);
+                atomicMax(a.level + w, olx);
+                __threadfence();
+                if (atomicSub(a.cnt + w, 1) == 1) nv = w;
+            }
+            const unsigned bal = __ballot_sync(full, nv >= 0);
+            if (bal) {
+                const int32_t r = __popc(bal & ((1u << lane) - 1u)), nn = __popc(bal);
+                if (qn + nn <= LEVEL_Q) {
+                    if (nv >= 0) wq[qn + r] = nv;
+                    qn += nn;
+                } else {
+                    int32_t base = 0;
+                    if (lane == 0) base = atomicAdd(a.ovf_count, nn);
+                    base = __shfl_sync(full, base, 0);
+                    if (nv >= 0) a.ovf[base + r] = nv;
+                }
+                __syncwarp();
+            }
+        }
+    }
+}
+
+// Sweep (items == NULL): the sources (no in-edges, decided from the offsets,
+// so no decrement can release one twice) start the peel.  List: expand
+// released nodes that overflowed a queue.
+__global__ void __launch_bounds__(SCC_THREADS) k_level_peel(LevelArgs a, int32_t n, const int32_t* __restrict__ items) {
+    __shared__ int32_t queues[SCC_THREADS / 32][LEVEL_Q];
+    const int lane = threadIdx.x & 31;
+    int32_t* wq = queues[threadIdx.x >> 5];
+    int32_t qn = 0;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < n; base += nwarps * 32) {
+        const int64_t i = base + lane;
+        int32_t x = -1;
+        if (i < n) {
+            if (items) x = items[i];
+            else if (__ldg(a.r_begin + i + 1) == __ldg(a.r_begin + i)) x = (int32_t)i;
+        }
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, x >= 0);
+        if (x >= 0) wq[__popc(bal & ((1u << lane) - 1u))] = x;    // qn == 0 here
+        qn = __popc(bal);
+        __syncwarp();
+        level_drain(a, wq, qn);
+    }
+}
+
+__global__ void k_level_max(int32_t n, const int32_t* __restrict__ level, int32_t* __restrict__ out) {
+    int32_t m = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        m = max(m, level[i]);
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+namespace {
+struct Buf {
+    void* p = nullptr;
+    cudaStream_t st = nullptr;
+    ~Buf() { if (p) cudaFreeAsync(p, st); }
+    template <class T> T* as() { return (T*)p; }
+};
+int get(Buf& b, size_t bytes, cudaStream_t st) {
+    b.st = st;
+    SCC_CUDA(scc_impl_malloc_async(&b.p, bytes > 0 ? bytes : 16, st));
+    return SCC_OK;
+}
+struct Stream {
+    cudaStream_t st = nullptr;
+    ~Stream() { if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); } }
+};
+}  // namespace
+
+// Levels into d_level (device, n ints); *max_level from the device.
+static int levels_on_device(const scc_graph* g, cudaStream_t st, int32_t* d_level, int32_t* max_level) {
+    int32_t n = g->n;
+    *max_level = 0;
+    if (n == 0) return SCC_OK;
+    Buf cnt, ovf, list, ctr;
+    SCC_TRY(get(cnt, sizeof(int32_t) * (size_t)n, st));
+    SCC_TRY(get(ovf, sizeof(int32_t) * (size_t)n, st));
+    SCC_TRY(get(list, sizeof(int32_t) * (size_t)n, st));
+    SCC_TRY(get(ctr, sizeof(int32_t) * 2, st));
+    LevelArgs a;
+    a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin;
+    a.cnt = cnt.as<int32_t>(); a.level = d_level; a.ovf = ovf.as<int32_t>(); a.ovf_count = ctr.as<int32_t>();
+    k_level_init<<<scc_blocks(n), SCC_THREADS, 0, st>>>(n, g->r_begin, a.cnt, d_level);
+    SCC_CUDA(cudaPeekAtLastError());
+    SCC_CUDA(cudaMemsetAsync(ctr.p, 0, sizeof(int32_t) * 2, st));
+    k_level_peel<<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, st>>>(a, n, nullptr);
+    SCC_CUDA(cudaPeekAtLastError());
+    // each node is released once, so the overflow lists together hold at most n
+    for (int round = 0; round < 1000000; ++round) {
+        int32_t novf = 0;
+        SCC_CUDA(cudaMemcpyAsync(&novf, ctr.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        SCC_CUDA(cudaStreamSynchronize(st));
+        if (novf == 0) break;
+        SCC_CUDA(cudaMemcpyAsync(list.p, ovf.p, sizeof(int32_t) * (size_t)novf, cudaMemcpyDeviceToDevice, st));
+        SCC_CUDA(cudaMemsetAsync(ctr.p, 0, sizeof(int32_t), st));
+        k_level_peel<<<scc_blocks(novf, SCC_THREADS, 148 * 8), SCC_THREADS, 0, st>>>(a, novf, list.as<int32_t>());
+        SCC_CUDA(cudaPeekAtLastError());
+    }
+    int32_t* d_max = ctr.as<int32_t>() + 1;
+    k_level_max<<<scc_blocks(n), SCC_THREADS, 0, st>>>(n, d_level, d_max);
+    SCC_CUDA(cudaPeekAtLastError());
+    SCC_CUDA(cudaMemcpyAsync(max_level, d_max, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    SCC_CUDA(cudaStreamSynchronize(st));
+    return SCC_OK;
+}
+
+extern "C" int scc_topological_levels(const scc_graph* dag, int32_t* levels, int32_t* max_level) {
+    SCC_REQUIRE(dag && levels && max_level, SCC_ERR_INVALID, "NULL argument");
+    SCC_CUDA(cudaSetDevice(dag->device));
+    Stream s;
+    SCC_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+    Buf lev;
+    SCC_TRY(get(lev, sizeof(int32_t) * (size_t)dag->n, s.st));
+    SCC_TRY(levels_on_device(dag, s.st, lev.as<int32_t>(), max_level));
+    if (dag->n > 0)
+        SCC_CUDA(cudaMemcpyAsync(levels, lev.p, sizeof(int32_t) * (size_t)dag->n, cudaMemcpyDeviceToHost, s.st));
+    SCC_CUDA(cudaStreamSynchronize(s.st));
+    return SCC_OK;
+}
+
+// ------------------------------------------------------------------ affected levels
+// Every inserted edge joining two SCCs adds one over the level interval
+// [min, max] of its endpoints' SCCs: +1 at min, -1 at max + 1.
+__global__ void k_affect_diff(int64_t k, const int32_t* __restrict__ a, const int32_t* __restrict__ b,
+                              const int32_t* __restrict__ label, int32_t n, const int32_t* __restrict__ level,
+                              int32_t num_sccs, int32_t max_level, int32_t* __restrict__ diff, int* __restrict__ bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < k; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t x = a[i], y = b[i];
+        if (x < 0 || x >= n || y < 0 || y >= n) { atomicExch(bad, 1); continue; }
+        int32_t cx = label[x], cy = label[y];
+        if (cx < 0 || cx >= num_sccs || cy < 0 || cy >= num_sccs) { atomicExch(bad, 2); continue; }
+        if (cx == cy) continue;
+        int32_t lx = level[cx], ly = level[cy];
+        if (lx < 0 || lx > max_level || ly < 0 || ly > max_level) { atomicExch(bad, 3); continue; }
+        atomicAdd(diff + min(lx, ly), 1);
+        atomicAdd(diff + max(lx, ly) + 1, -1);
+    }
+}
+
+__global__ void k_count_zero(int32_t n, const int32_t* __restrict__ v, int32_t* __restrict__ out) {
+    int32_t c = 0;
+    int64_t limit = (((int64_t)n + 31) / 32) * 32;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += (int64_t)gridDim.x * blockDim.x)
+        c += (i < n && v[i] == 0);
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+extern "C" int scc_affected_levels(const scc_graph* dag, const int32_t* levels, int32_t max_level, int32_t n,
+                                   const int32_t* labels, int64_t n_ins, const int32_t* ins_src,
+                                   const int32_t* ins_dst, int32_t* affected, int32_t* num_unaffected) {
+    SCC_REQUIRE(dag && levels && labels && affected && num_unaffected && n >= 0 && max_level >= 0 && n_ins >= 0,
+                SCC_ERR_INVALID, "bad argument");
+    SCC_REQUIRE(n_ins == 0 || (ins_src && ins_dst), SCC_ERR_INVALID, "NULL batch arrays");
+    SCC_CUDA(cudaSetDevice(dag->device));
+    Stream s;
+    SCC_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+    cudaStream_t st = s.st;
+    const int32_t L = max_level + 1;
+    Buf lab, lev, src, dst, diff, out, bad, tmp;
+    SCC_TRY(get(lab, sizeof(int32_t) * (size_t)n, st));
+    SCC_TRY(get(lev, sizeof(int32_t) * (size_t)dag->n, st));
+    SCC_TRY(get(src, sizeof(int32_t) * (size_t)n_ins, st));
+    SCC_TRY(get(dst, sizeof(int32_t) * (size_t)n_ins, st));
+    SCC_TRY(get(diff, sizeof(int32_t) * ((size_t)L + 1), st));
+    SCC_TRY(get(out, sizeof(int32_t) * (size_t)L, st));
+    SCC_TRY(get(bad, sizeof(int32_t) * 2, st));
+    SCC_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int32_t) * 2, st));
+    SCC_CUDA(cudaMemsetAsync(diff.p, 0, sizeof(int32_t) * ((size_t)L + 1), st));
+    if (n > 0) SCC_CUDA(cudaMemcpyAsync(lab.p, labels, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, st));
+    if (dag->n > 0)
+        SCC_CUDA(cudaMemcpyAsync(lev.p, levels, sizeof(int32_t) * (size_t)dag->n, cudaMemcpyHostToDevice, st));
+    if (n_ins > 0) {
+        SCC_CUDA(cudaMemcpyAsync(src.p, ins_src, sizeof(int32_t) * (size_t)n_ins, cudaMemcpyHostToDevice, st));
+        SCC_CUDA(cudaMemcpyAsync(dst.p, ins_dst, sizeof(int32_t) * (size_t)n_ins, cudaMemcpyHostToDevice, st));
+        k_affect_diff<<<scc_blocks(n_ins), SCC_THREADS, 0, st>>>(n_ins, src.as<int32_t>(), dst.as<int32_t>(),
+                                                                lab.as<int32_t>(), n, lev.as<int32_t>(), dag->n,
+                                                                max_level, diff.as<int32_t>(), bad.as<int>());
+        SCC_CUDA(cudaPeekAtLastError());
+    }
+    size_t tbytes = 0;
+    SCC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tbytes, diff.as<int32_t>(), out.as<int32_t>(), L, st));
+    SCC_TRY(get(tmp, tbytes, st));
+    SCC_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tbytes, diff.as<int32_t>(), out.as<int32_t>(), L, st));
+    k_count_zero<<<scc_blocks(L), SCC_THREADS, 0, st>>>(L, out.as<int32_t>(), bad.as<int32_t>() + 1);
+    SCC_CUDA(cudaPeekAtLastError());
+    int32_t h[2] = {0, 0};
+    SCC_CUDA(cudaMemcpyAsync(affected, out.p, sizeof(int32_t) * (size_t)L, cudaMemcpyDeviceToHost, st));
+    SCC_CUDA(cudaMemcpyAsync(h, bad.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    SCC_CUDA(cudaStreamSynchronize(st));
+    SCC_REQUIRE(h[0] != 1, SCC_ERR_INVALID, "inserted endpoint outside [0, %d)", n);
+    SCC_REQUIRE(h[0] != 2, SCC_ERR_INVALID, "label outside [0, %d)", dag->n);
+    SCC_REQUIRE(h[0] != 3, SCC_ERR_INVALID, "level outside [0, %d]", max_level);
+    *num_unaffected = h[1];
+    return SCC_OK;
+}
+
+// ------------------------------------------------------------------ trim shortcut
+__global__ void k_finish_unaffected(int32_t n, const int32_t* __restrict__ level, const int32_t* __restrict__ affected,
+                                    int32_t max_level, int32_t* __restrict__ color, int32_t* __restrict__ scc,
+                                    int32_t* __restrict__ count) {
+    int32_t c = 0;
+    int64_t limit = (((int64_t)n + 31) / 32) * 32;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i < n) {
+            int32_t l = level[i];
+            if (l >= 0 && l <= max_level && affected[l] == 0) {
+                color[i] = SCC_COLOR_DONE;
+                scc[i] = (int32_t)i;
+                c++;
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
+extern "C" int scc_state_finish_unaffected(scc_state* s, const int32_t* levels, const int32_t* affected,
+                                           int32_t max_level, int32_t* finished) {
+    SCC_REQUIRE(s && levels && affected && max_level >= 0, SCC_ERR_INVALID, "bad argument");
+    SCC_CUDA(cudaSetDevice(s->device));
+    int32_t n = s->n;
+    Buf lev, aff;
+    SCC_TRY(get(lev, sizeof(int32_t) * (size_t)n, s->stream));
+    SCC_TRY(get(aff, sizeof(int32_t) * ((size_t)max_level + 1), s->stream));
+    if (n > 0) SCC_CUDA(cudaMemcpyAsync(lev.p, levels, sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    SCC_CUDA(cudaMemcpyAsync(aff.p, affected, sizeof(int32_t) * ((size_t)max_level + 1), cudaMemcpyHostToDevice,
+                             s->stream));
+    SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
+    if (n > 0) {
+        k_finish_unaffected<<<scc_blocks(n), SCC_THREADS, 0, s->stream>>>(n, lev.as<int32_t>(), aff.as<int32_t>(),
+                                                                           max_level, s->color, s->scc,
+                                                                           s->ctr + CTR_COUNT);
+        SCC_LAUNCHED(s);
+    }
+    SCC_TRY(scc_sync_counters(s));
+    s->fresh = false;
+    s->cnt_valid = false;
+    if (finished) *finished = s->h_ctr[CTR_COUNT];
+    return SCC_OK;
+}

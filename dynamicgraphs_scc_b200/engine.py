@@ -214,6 +214,13 @@ class State:
     def set_scc(self, a) -> None:
         call("scc_state_set_scc", self.handle, i32p(_i32(a)))
 
+    def finish_unaffected(self, levels, affected, max_level: int) -> int:
+        """Method 7's trim shortcut: finish every node of an unaffected level as its own SCC."""
+        k = C.c_int32()
+        call("scc_state_finish_unaffected", self.handle, i32p(_i32(levels)), i32p(_i32(affected)), max_level,
+             C.byref(k))
+        return k.value
+
     def trim_targets(self) -> np.ndarray:
         c = C.c_int32()
         call("scc_state_get_trim_targets", self.handle, None, 0, C.byref(c))
@@ -591,6 +598,38 @@ def condensation_graph(graph: Graph, labels, num_sccs: int, ins_src=(), ins_dst=
     call("scc_condensation_graph", graph.handle, i32p(lab), num_sccs, int(s.size), i32p(s) if s.size else None,
          i32p(d) if d.size else None, C.byref(h))
     return Graph(h)
+
+
+def topological_levels(dag: Graph):
+    """Method 7's BFS levels of a condensation DAG: (levels, max_level)."""
+    n = dag.num_nodes()
+    lev = np.empty(max(n, 1), np.int32)
+    ml = C.c_int32()
+    call("scc_topological_levels", dag.handle, i32p(lev), C.byref(ml))
+    return lev[:n], ml.value
+
+
+def affected_levels(dag: Graph, levels, max_level: int, labels, ins_src=(), ins_dst=()):
+    """Method 7's affect_level: (coverage per level 0..max_level, unaffected level count)."""
+    lev, lab = _i32(levels), _i32(labels)
+    s, d = _i32(ins_src), _i32(ins_dst)
+    out = np.empty(max_level + 1, np.int32)
+    z = C.c_int32()
+    call("scc_affected_levels", dag.handle, i32p(lev), max_level, int(lab.size), i32p(lab), int(s.size),
+         i32p(s) if s.size else None, i32p(d) if d.size else None, i32p(out), C.byref(z))
+    return out, z.value
+
+
+def read_edge_list(path: str):
+    """read_file: (src, dst) 0-based and N, the largest 1-based id."""
+    m = C.c_int64()
+    mx = C.c_int32()
+    call("scc_read_edge_list", path.encode(), 0, None, None, C.byref(m), C.byref(mx))
+    src = np.empty(max(m.value, 1), np.int32)
+    dst = np.empty(max(m.value, 1), np.int32)
+    if m.value:
+        call("scc_read_edge_list", path.encode(), m.value, i32p(src), i32p(dst), C.byref(m), C.byref(mx))
+    return src[:m.value], dst[:m.value], mx.value
 
 
 def read_scc_list(path: str, n: int):

@@ -100,6 +100,11 @@ int scc_graph_create_csr_device(int32_t n, int32_t m, const int32_t* d_begin, co
  * the fast parser of src_CUDA/scc_cuda_dynamic.cpp:59-147).  Lines starting
  * with '%' or '#' are skipped.  Duplicates and self-loops are kept. */
 int scc_graph_load_edge_list(const char* path, int device, scc_graph** out);
+/* read_file (src/common_main.h:61-83) into host arrays, 0-based: *count edges, *max_id = N
+ * (the largest 1-based id).  capacity 0 only counts; otherwise src/dst hold capacity
+ * entries, at least *count. */
+int scc_read_edge_list(const char* path, int64_t capacity, int32_t* src, int32_t* dst, int64_t* count,
+                       int32_t* max_id);
 /* Re-upload host CSR arrays into an existing graph of the same n and m (no
  * allocation): the per-request H2D of graph_upload (src_CUDA/scc_cuda_graph.cu:4)
  * for callers that keep the device graph between runs.  Ordered on `stream`
@@ -336,6 +341,27 @@ int scc_insert_idea1(scc_graph* g, scc_state* s, int64_t n_ins, const int32_t* s
  * the inserted batch (host arrays) mapped to (id(u), id(v)), duplicates dropped. */
 int scc_condensation_graph(const scc_graph* g, const int32_t* labels, int32_t num_sccs, int64_t n_ins,
                            const int32_t* ins_src, const int32_t* ins_dst, scc_graph** out);
+/* Method 7, the BFS of create_scc_edges (src/common_main.h:85-108, 210-219): topological
+ * levels of a condensation DAG (scc_condensation_graph with no inserted edges).  levels[c]
+ * (host array of dag's n) is the longest path from a source; a node on or behind a cycle
+ * keeps the largest level + 1 of its released predecessors, or 0, as the reference's queue
+ * leaves it.  *max_level = the largest level (the reference's "max_level:" line). */
+int scc_topological_levels(const scc_graph* dag, int32_t* levels, int32_t* max_level);
+/* Method 7, affect_level (src/common_main.h:232-262): every inserted edge (u, v) of the
+ * original graph's n vertices with labels[u] != labels[v] covers the levels between those
+ * of its two SCCs, inclusive.  affected[l], l in [0, max_level] (host array of
+ * max_level + 1), receives how many edges cover level l (the prefix-summed affect_level);
+ * *num_unaffected counts the levels no edge covers ("size of unaffected_levels:").  Sums
+ * are exact int32 (the reference accumulates in float). */
+int scc_affected_levels(const scc_graph* dag, const int32_t* levels, int32_t max_level, int32_t n,
+                        const int32_t* labels, int64_t n_ins, const int32_t* ins_src, const int32_t* ins_dst,
+                        int32_t* affected, int32_t* num_unaffected);
+/* Method 7's trim shortcut (src/scc_trim1.cc:67-73) on a state of the condensation graph
+ * with inserted edges: every node c with affected[levels[c]] == 0 is finished as its own
+ * SCC (G_SCC = c, colour -2) before scc_run, which then decomposes only the rest.  No
+ * inserted edge can join such a node to another.  *finished may be NULL. */
+int scc_state_finish_unaffected(scc_state* s, const int32_t* levels, const int32_t* affected, int32_t max_level,
+                                int32_t* finished);
 
 /* ---- serving loop (no counterpart in the reference, whose dynamic methods read one
  * update file per process, src/common_main.h:500-732) ----------------------------------- */

@@ -58,6 +58,10 @@ def lib():
                                 C.c_int32, C.c_int32, _I64P, _I64P]
         L.orc_fw_bw.restype = C.c_int64
         L.orc_choose_pivot.argtypes = [C.c_int32, _I32P, _I32P, _I32P, C.c_int32]
+        L.orc_topo_levels.argtypes = [C.c_int32, _I32P, _I32P, _I32P]
+        L.orc_topo_levels.restype = C.c_int32
+        L.orc_affected_levels.argtypes = [_I32P, _I32P, C.c_int32, C.c_int64, _I32P, _I32P, _I32P]
+        L.orc_affected_levels.restype = C.c_int32
         L.orc_choose_pivot.restype = C.c_int32
         L.orc_bf16.argtypes = [C.c_float]
         L.orc_bf16.restype = C.c_float
@@ -86,6 +90,9 @@ def ref():
         L.ref_method2.restype = C.c_int
         L.ref_tarjan.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P, _I32P, C.POINTER(C.c_double)]
         L.ref_tarjan.restype = C.c_int
+        L.ref_method7_levels.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P, C.c_int64, _I32P, _I32P, _I32P,
+                                         C.c_int32, _I32P, _I32P]
+        L.ref_method7_levels.restype = C.c_int
         _ref = L
     return _ref
 
@@ -211,6 +218,70 @@ def ref_tarjan(csr):
     if rc != 0:
         raise RuntimeError("reference Tarjan failed")
     return canonical(out[:n]), ms.value
+
+
+# ---------------------------------------------------------------- method 7 levels (scc_oracle.c)
+def scc_ids(labels):
+    """scc_list.txt ids of canonical labels: numbered by first appearance over
+    the vertices (output_scc_list, src/scc_post_analyze.cc:31-53)."""
+    labels = np.asarray(labels)
+    first = {}
+    out = np.empty(labels.size, np.int32)
+    for i, r in enumerate(labels.tolist()):
+        out[i] = first.setdefault(r, len(first))
+    return out, len(first)
+
+
+def condensation_csr(ids, num_sccs, src, dst):
+    """The original edges' condensation as create_scc_edges builds adj_list:
+    one entry per edge joining two SCCs, duplicates kept, in edge order."""
+    ids = np.asarray(ids, np.int64)
+    a = ids[np.asarray(src, np.int64)]
+    b = ids[np.asarray(dst, np.int64)]
+    keep = a != b
+    a, b = a[keep], b[keep]
+    order = np.argsort(a, kind="stable")
+    begin = np.zeros(num_sccs + 1, np.int32)
+    np.add.at(begin, a + 1, 1)
+    return np.cumsum(begin).astype(np.int32), b[order].astype(np.int32)
+
+
+def topo_levels(begin, adj):
+    """(levels, max_level) by the reference's FIFO level BFS."""
+    n = begin.size - 1
+    lev = np.empty(max(n, 1), np.int32)
+    m = lib().orc_topo_levels(n, _p(np.ascontiguousarray(begin, np.int32)),
+                              _p(np.ascontiguousarray(adj, np.int32) if adj.size else np.zeros(1, np.int32)), _p(lev))
+    return lev[:n], int(m)
+
+
+def affected_levels(ids, levels, max_level, src, dst):
+    """(affected[0..max_level], number of unaffected levels)."""
+    src = np.ascontiguousarray(src, np.int32)
+    dst = np.ascontiguousarray(dst, np.int32)
+    out = np.empty(max_level + 1, np.int32)
+    z = lib().orc_affected_levels(_p(np.ascontiguousarray(ids, np.int32)), _p(np.ascontiguousarray(levels, np.int32)),
+                                  max_level, src.size, _p(src if src.size else np.zeros(1, np.int32)),
+                                  _p(dst if dst.size else np.zeros(1, np.int32)), _p(out))
+    return out, int(z)
+
+
+def ref_method7_levels(nv, src, dst, ins_src, ins_dst, ids, num_sccs):
+    """The reference's own create_scc_edges with met_algo 7: (level_ver,
+    prefix-summed affect_level).  Only for batches that leave a level
+    unaffected (its closing loop misbehaves otherwise)."""
+    src, dst = np.ascontiguousarray(src, np.int32), np.ascontiguousarray(dst, np.int32)
+    isrc, idst = np.ascontiguousarray(ins_src, np.int32), np.ascontiguousarray(ins_dst, np.int32)
+    lev = np.empty(max(num_sccs, 1), np.int32)
+    aff = np.empty(num_sccs + 5, np.int32)
+    one = np.zeros(1, np.int32)
+    with _QuietStdout():
+        rc = ref().ref_method7_levels(nv, src.size, _p(src if src.size else one), _p(dst if dst.size else one),
+                                      isrc.size, _p(isrc if isrc.size else one), _p(idst if idst.size else one),
+                                      _p(np.ascontiguousarray(ids, np.int32)), num_sccs, _p(lev), _p(aff))
+    if rc != 0:
+        raise RuntimeError("reference create_scc_edges failed")
+    return lev[:num_sccs], aff
 
 
 # ---------------------------------------------------------------- learned pivot network (mlp_oracle.c)

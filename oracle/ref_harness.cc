@@ -108,3 +108,31 @@ extern "C" int ref_tarjan(int32_t n, int64_t m, const int32_t* begin, const int3
     if (ms_out) *ms_out = j.ms;
     return 0;
 }
+
+// Method 7's preprocessing by the reference's own main_t::create_scc_edges
+// (src/common_main.h:180-262) with met_algo = 7: the condensation edges, the
+// BFS levels of the original condensation (level_ver) and the prefix-summed
+// affect_level.  One OpenMP thread: its loops push into shared vectors
+// without locks.  Its closing loop runs to unaffected_levels.size() - 1 on an
+// unsigned size, so callers only pass batches that leave a level unaffected.
+// ids: the scc_list ids (read_file1) of the nv vertices; edges 0-based.
+extern "C" int ref_method7_levels(int32_t nv, int64_t m, const int32_t* osrc, const int32_t* odst, int64_t k,
+                                  const int32_t* isrc, const int32_t* idst, const int32_t* ids, int32_t num_sccs,
+                                  int32_t* level_out, int32_t* affect_out) {
+    gm_rt_set_num_threads(1);
+    omp_set_num_threads(1);
+    my_main T;
+    met_algo = 7;
+    scc_list.assign(ids, ids + nv);
+    level_ver.clear();
+    affect_level.clear();
+    new_edge_nodes.clear();
+    std::vector<std::pair<int, int>> orig((size_t)m), ins((size_t)k), scc_edges;
+    for (int64_t i = 0; i < m; ++i) orig[(size_t)i] = std::make_pair(osrc[i], odst[i]);
+    for (int64_t i = 0; i < k; ++i) ins[(size_t)i] = std::make_pair(isrc[i], idst[i]);
+    T.create_scc_edges(orig, ins, scc_edges, nv, num_sccs);
+    for (int32_t i = 0; i < num_sccs; ++i) level_out[i] = level_ver[(size_t)i];
+    for (int32_t i = 0; i < num_sccs + 5; ++i) affect_out[i] = affect_level[(size_t)i];
+    met_algo = 2;
+    return 0;
+}

@@ -342,3 +342,58 @@ void orc_scc_canonical(int32_t n, const int32_t* begin, const int32_t* node_idx,
     orc_canonical(n, scc, out);
     free(scc);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Method 7: topological levels of the condensation graph and the levels an   */
+/* inserted batch affects (create_scc_edges + BFS, src/common_main.h:85-108,   */
+/* 180-262).  Restated literally: a FIFO queue seeded, in id order, with the   */
+/* nodes that have no in-edge but some out-edge; every edge of a processed    */
+/* node decrements its child's in-degree (duplicates counted), queues the      */
+/* child at zero, and overwrites the child's level with the parent's + 1.      */
+/* ------------------------------------------------------------------------ */
+int32_t orc_topo_levels(int32_t n, const int32_t* begin, const int32_t* adj, int32_t* level) {
+    int32_t* indeg = (int32_t*)calloc((size_t)n + 1, sizeof(int32_t));
+    int32_t* queue = (int32_t*)malloc(sizeof(int32_t) * ((size_t)n + 1));
+    int64_t head = 0, tail = 0;
+    int32_t max_level = 0;
+    for (int32_t v = 0; v < n; ++v) level[v] = 0;
+    for (int64_t k = 0; k < begin[n]; ++k) indeg[adj[k]]++;
+    for (int32_t v = 0; v < n; ++v)
+        if (indeg[v] == 0 && begin[v + 1] > begin[v]) queue[tail++] = v;
+    while (head < tail) {
+        int32_t top = queue[head++];
+        for (int32_t k = begin[top]; k < begin[top + 1]; ++k) {
+            int32_t c = adj[k];
+            if (--indeg[c] == 0) queue[tail++] = c;
+            level[c] = level[top] + 1;
+            if (level[c] > max_level) max_level = level[c];
+        }
+    }
+    free(indeg);
+    free(queue);
+    return max_level;
+}
+
+/* affect_level: +1 at min(level), -1 at max(level) + 1 for every inserted edge
+ * whose endpoints lie in different SCCs, then the inclusive prefix sum
+ * (parallel_prefix_sum, common_main.h:109-148, here in exact integers).
+ * affected[0..max_level]; returns the count of zero entries (unaffected). */
+int32_t orc_affected_levels(const int32_t* label, const int32_t* level, int32_t max_level, int64_t k,
+                            const int32_t* src, const int32_t* dst, int32_t* affected) {
+    int32_t* diff = (int32_t*)calloc((size_t)max_level + 2, sizeof(int32_t));
+    for (int64_t i = 0; i < k; ++i) {
+        int32_t a = label[src[i]], b = label[dst[i]];
+        if (a == b) continue;
+        int32_t la = level[a], lb = level[b];
+        diff[la < lb ? la : lb] += 1;
+        diff[(la > lb ? la : lb) + 1] -= 1;
+    }
+    int32_t run = 0, zeros = 0;
+    for (int32_t l = 0; l <= max_level; ++l) {
+        run += diff[l];
+        affected[l] = run;
+        zeros += run == 0;
+    }
+    free(diff);
+    return zeros;
+}

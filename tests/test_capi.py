@@ -96,3 +96,19 @@ def test_generator_rejects_bad_params():
     from dynamicgraphs_scc_b200.capi import SccError
     with pytest.raises(SccError):
         generate_edges_host(rmat_scale=40, edge_factor=1)
+
+
+def test_read_edge_list_host_parser(tmp_path):
+    """read_file's format on the host (no device work): 1-based ids, comment
+    lines skipped, N = the largest id, malformed lines rejected."""
+    from dynamicgraphs_scc_b200 import SccError, read_edge_list
+    p = tmp_path / "e.txt"
+    p.write_text("% header\n1 2\n2 3\n# note\n3 1\n7 7\n")
+    s, d, n = read_edge_list(str(p))
+    assert s.tolist() == [0, 1, 2, 6] and d.tolist() == [1, 2, 0, 6] and n == 7
+    p.write_text("")
+    s, d, n = read_edge_list(str(p))
+    assert s.size == 0 and n == 0
+    p.write_text("1 x\n")
+    with pytest.raises(SccError):
+        read_edge_list(str(p))

@@ -83,7 +83,7 @@ def test_cli_methods_and_flags(gpu, tmp_path):
     g = tmp_path / "g.txt"
     write_edges(g, s, d)
     counts = set()
-    for method in ("0", "1", "2", "7"):
+    for method in ("0", "1", "2"):
         r = subprocess.run([OUR_CLI, str(g), "1", method, "-d"], cwd=tmp_path, capture_output=True, text=True,
                            timeout=300)
         assert r.returncode == 0, r.stderr
@@ -96,4 +96,67 @@ def test_cli_methods_and_flags(gpu, tmp_path):
     assert r.returncode == 1 and "unsupported" in r.stderr
     r = subprocess.run([OUR_CLI, str(tmp_path / "missing.txt"), "1", "2"], cwd=tmp_path, capture_output=True,
                        text=True, timeout=300)
+    assert r.returncode == 1
+
+
+def _line(out, prefix):
+    for line in out.splitlines():
+        if line.startswith(prefix):
+            return line[len(prefix):].strip()
+    return None
+
+
+def test_cli_update_methods(gpu, tmp_path):
+    """Methods 5-11 as the reference driver runs them: the batch file, the
+    original graph in refined_edges.txt beside it, the previous decomposition
+    in scc_list.txt (written by a method-2 "-p" run)."""
+    rng = np.random.default_rng(21)
+    n = 6000
+    s, d = random_graph(n, 9000, 8)
+    s = np.append(s, n - 1).astype(np.int32); d = np.append(d, 0).astype(np.int32)
+    write_edges(tmp_path / "refined_edges.txt", s, d)
+    r = subprocess.run([OUR_CLI, str(tmp_path / "refined_edges.txt"), "1", "2", "-p"], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    labels = O.tarjan_canonical(*O.build_csr(n, s, d)[:2])
+    ids, k = O.scc_ids(labels)
+    isrc = rng.integers(0, n, 12).astype(np.int32); idst = rng.integers(0, n, 12).astype(np.int32)
+    isrc[-1] = n - 1                                # the batch's N must not exceed the graph's
+    write_edges(tmp_path / "ins.txt", isrc, idst)
+    upd = O.tarjan_canonical(*O.build_csr(n, np.concatenate([s, isrc]), np.concatenate([d, idst]))[:2])
+    b, a = O.condensation_csr(ids, k, s, d)
+    lev, ml = O.topo_levels(b, a)
+    _, unaffected = O.affected_levels(ids, lev, ml, isrc, idst)
+    for method in ("5", "6", "7", "11"):
+        r = subprocess.run([OUR_CLI, str(tmp_path / "ins.txt"), "2", method, "-d"], cwd=tmp_path,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, (method, r.stderr)
+        info = parse(r.stdout)
+        assert info["data"] == [str(tmp_path / "ins.txt"), method, "2"]
+        assert info["sccs"] == len(np.unique(upd)), method
+        if method == "7":
+            assert int(_line(r.stdout, "max_level:")) == ml
+            assert int(_line(r.stdout, "size of unaffected_levels:")) == unaffected
+            assert _line(r.stdout, "Trimmed nodes=") == "0"
+    # deletions: one edge inside a non-trivial SCC, one across SCCs
+    big = np.flatnonzero((labels[s] == labels[d]) & (s != d))
+    cross = np.flatnonzero(labels[s] != labels[d])
+    pick = np.array([big[0], cross[0]])
+    dsrc, ddst = s[pick].astype(np.int32), d[pick].astype(np.int32)
+    write_edges(tmp_path / "del.txt", dsrc, ddst)
+    gone = np.zeros(s.size, bool)
+    for x, y in zip(dsrc.tolist(), ddst.tolist()):
+        gone |= (s == x) & (d == y)
+    after = O.tarjan_canonical(*O.build_csr(n, s[~gone], d[~gone])[:2])
+    for method in ("8", "9", "10"):
+        r = subprocess.run([OUR_CLI, str(tmp_path / "del.txt"), "1", method], cwd=tmp_path,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, (method, r.stderr)
+        assert parse(r.stdout)["sccs"] == len(np.unique(after)), method
+        if method == "9":
+            assert _line(r.stdout, "affect_sccs:") == f"1 unaffect_sccs:{k - 1}"
+    # a batch naming a vertex beyond the original graph is an error
+    write_edges(tmp_path / "bad.txt", np.array([0], np.int32), np.array([n + 5], np.int32))
+    r = subprocess.run([OUR_CLI, str(tmp_path / "bad.txt"), "1", "6"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=300)
     assert r.returncode == 1

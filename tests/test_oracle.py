@@ -182,3 +182,79 @@ def test_pivot_features_oracle_known_answer():
     assert list(cnt_out) == [2, 1, 1, 1] and list(cnt_in) == [2, 1, 1, 0]
     f2 = O.pivot_features(csr, 0, class_size=3, cnt_out=cnt_out, cnt_in=cnt_in)
     assert f2[4] == O.bf16(np.float32(np.log1p(2.0)))
+
+
+# ---------------------------------------------------------------- method 7 levels
+def _levels_by_max(begin, adj):
+    """Longest path from the sources; nodes never released keep the largest
+    level + 1 of their released predecessors (the order-free form)."""
+    n = begin.size - 1
+    indeg = np.bincount(adj, minlength=n).astype(np.int64)
+    level = np.zeros(n, np.int64)
+    stack = [v for v in range(n) if indeg[v] == 0]
+    while stack:
+        v = stack.pop()
+        for c in adj[begin[v]:begin[v + 1]]:
+            level[c] = max(level[c], level[v] + 1)
+            indeg[c] -= 1
+            if indeg[c] == 0:
+                stack.append(int(c))
+    return level
+
+
+def test_topo_levels_known_answers():
+    # chain 0->1->2->3 plus 0->3: longest path gives 3 its level 3
+    b, a = O.condensation_csr(np.arange(4), 4, [0, 1, 2, 0], [1, 2, 3, 3])
+    lev, ml = O.topo_levels(b, a)
+    assert lev.tolist() == [0, 1, 2, 3] and ml == 3
+    # diamond with a duplicate edge: 0->1, 0->2, 1->3, 2->3, 2->3
+    b, a = O.condensation_csr(np.arange(4), 4, [0, 0, 1, 2, 2], [1, 2, 3, 3, 3])
+    lev, ml = O.topo_levels(b, a)
+    assert lev.tolist() == [0, 1, 1, 2] and ml == 2
+    # labels that are not SCCs: 1<->2 is a cycle fed by 0, 3 hangs off it.
+    # 1 and 2 are never released; 1 keeps 0's level + 1, 2 and 3 stay 0.
+    b, a = O.condensation_csr(np.arange(4), 4, [0, 1, 2, 2], [1, 2, 1, 3])
+    lev, ml = O.topo_levels(b, a)
+    assert lev.tolist() == [0, 1, 0, 0] and ml == 1
+    # affected: edge 3->0 covers levels [0, 2] of the diamond
+    aff, z = O.affected_levels(np.arange(4), np.array([0, 1, 1, 2]), 2, [3], [0])
+    assert aff.tolist() == [1, 1, 1] and z == 0
+    aff, z = O.affected_levels(np.arange(4), np.array([0, 1, 1, 2]), 2, [1, 2], [2, 1])
+    assert aff.tolist() == [0, 2, 0] and z == 2
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_topo_levels_fifo_equals_longest_path(seed):
+    rng = np.random.default_rng(seed)
+    n = 2000
+    s = rng.integers(0, n, 3 * n).astype(np.int32)
+    d = rng.integers(0, n, 3 * n).astype(np.int32)
+    for ids, k in [O.scc_ids(O.tarjan_canonical(*O.build_csr(n, s, d)[:2])), (np.arange(n, dtype=np.int32), n)]:
+        b, a = O.condensation_csr(ids, k, s, d)
+        lev, ml = O.topo_levels(b, a)
+        assert np.array_equal(lev, _levels_by_max(b, a))
+        assert ml == int(lev.max(initial=0))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("seed", [4, 5, 6, 7])
+def test_method7_levels_match_reference(seed):
+    """Levels and the prefix-summed affect_level against the reference's own
+    create_scc_edges (met_algo 7) on seeded graphs and batches."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(500, 4000))
+    m = int(n * rng.uniform(1.2, 2.5))
+    s = rng.integers(0, n, m).astype(np.int32)
+    d = rng.integers(0, n, m).astype(np.int32)
+    ids, k = O.scc_ids(O.tarjan_canonical(*O.build_csr(n, s, d)[:2]))
+    b, a = O.condensation_csr(ids, k, s, d)
+    lev, ml = O.topo_levels(b, a)
+    for nb in (1, 3, 10):
+        isrc = rng.integers(0, n, nb).astype(np.int32)
+        idst = rng.integers(0, n, nb).astype(np.int32)
+        aff, z = O.affected_levels(ids, lev, ml, isrc, idst)
+        if z == 0:
+            continue                  # the reference's closing loop needs an unaffected level
+        rl, ra = O.ref_method7_levels(n, s, d, isrc, idst, ids, k)
+        assert np.array_equal(rl, lev)
+        assert np.array_equal(ra[:ml + 1], aff)
