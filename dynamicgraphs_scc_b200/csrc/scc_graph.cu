@@ -12,6 +12,7 @@
 #include <stdarg.h>
 #include <stdlib.h>
 #include <string.h>
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include "scc_internal.cuh"
@@ -76,23 +77,46 @@ __global__ void k_make_keys(int64_t m, const int32_t* __restrict__ a, const int3
     if (local) atomicAdd(dropped, local);
 }
 
-// begin[v] = first index i with key[i]>>32 >= v, for v in [0, n]; keys sorted.
-__global__ void k_fill_offsets(int64_t m, int32_t n, const unsigned long long* __restrict__ keys,
-                               int32_t* __restrict__ begin) {
+// Offsets from sorted keys: begin[v] = first index i with key(i) >= v, for v
+// in [0, n].  Each key boundary fills at most FILL_SERIAL entries of the gap
+// before it; entries of longer gaps (ids with no edges, e.g. a vertex range no
+// edge of a chunk touches) stay at -1 and k_fill_gaps* finds them by binary
+// search, so no thread walks millions of entries alone.  begin is preset to -1.
+#define FILL_SERIAL 32
+
+__device__ __forceinline__ int64_t key_hi(const unsigned long long* keys, int64_t i) { return (int64_t)(keys[i] >> 32); }
+__device__ __forceinline__ int64_t key_hi(const int32_t* keys, int64_t i) { return (int64_t)keys[i]; }
+
+template <class K>
+__global__ void k_fill_offsets_t(int64_t m, int32_t n, const K* __restrict__ keys, int32_t* __restrict__ begin) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= m; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t prev = (i == 0) ? -1 : (int64_t)(keys[i - 1] >> 32);
-        int64_t cur = (i == m) ? (int64_t)n : (int64_t)(keys[i] >> 32);
-        for (int64_t v = prev + 1; v <= cur && v <= n; ++v) begin[v] = (int32_t)i;
+        int64_t prev = (i == 0) ? -1 : key_hi(keys, i - 1);
+        int64_t cur = (i == m) ? (int64_t)n : key_hi(keys, i);
+        int64_t last = min(min(cur, (int64_t)n), prev + FILL_SERIAL);
+        for (int64_t v = prev + 1; v <= last; ++v) begin[v] = (int32_t)i;
     }
 }
 
-// begin[v] = first index i with keys[i] >= v, for v in [0, n]; 32-bit keys sorted.
-__global__ void k_fill_offsets32(int64_t m, int32_t n, const int32_t* __restrict__ keys, int32_t* __restrict__ begin) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= m; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t prev = (i == 0) ? -1 : (int64_t)keys[i - 1];
-        int64_t cur = (i == m) ? (int64_t)n : (int64_t)keys[i];
-        for (int64_t v = prev + 1; v <= cur && v <= n; ++v) begin[v] = (int32_t)i;
+template <class K>
+__global__ void k_fill_gaps_t(int64_t m, int32_t n, const K* __restrict__ keys, int32_t* __restrict__ begin) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v <= n; v += (int64_t)gridDim.x * blockDim.x) {
+        if (begin[v] >= 0) continue;
+        int64_t lo = 0, hi = m;                  // first index with key >= v
+        while (lo < hi) {
+            int64_t mid = (lo + hi) >> 1;
+            if (key_hi(keys, mid) < v) lo = mid + 1; else hi = mid;
+        }
+        begin[v] = (int32_t)lo;
     }
+}
+
+template <class K>
+static cudaError_t fill_offsets(int64_t m, int32_t n, const K* keys, int32_t* begin, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(begin, 0xFF, sizeof(int32_t) * ((size_t)n + 1), st);
+    if (e != cudaSuccess) return e;
+    k_fill_offsets_t<K><<<scc_blocks(m + 1, 256, 148 * 64), 256, 0, st>>>(m, n, keys, begin);
+    k_fill_gaps_t<K><<<scc_blocks((int64_t)n + 1, 256, 148 * 64), 256, 0, st>>>(m, n, keys, begin);
+    return cudaPeekAtLastError();
 }
 
 __global__ void k_low_words(int64_t m, const unsigned long long* __restrict__ keys, int32_t* __restrict__ out) {
@@ -170,7 +194,7 @@ static int build_side(int32_t n, int64_t m, const int32_t* hi, const int32_t* lo
     int32_t *begin = nullptr, *idx = nullptr;
     SCC_CUDA(cudaMalloc(&begin, sizeof(int32_t) * ((size_t)n + 1)));
     SCC_CUDA(cudaMalloc(&idx, sizeof(int32_t) * (size_t)(mk > 0 ? mk : 1)));
-    k_fill_offsets<<<scc_blocks(mk + 1, 256, 148 * 64), 256, 0, st>>>(mk, n, sorted, begin);
+    SCC_CUDA(fill_offsets(mk, n, sorted, begin, st));
     SCC_CUDA(cudaPeekAtLastError());
     if (mk > 0) {
         k_low_words<<<scc_blocks(mk, 256, 148 * 64), 256, 0, st>>>(mk, sorted, idx);
@@ -247,8 +271,7 @@ static int transpose_into(scc_graph* g, cudaStream_t st) {
     SCC_CUDA(tmp.alloc(tb));
     SCC_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, g->node_idx, (int32_t*)keys.p, (const int32_t*)src.p,
                                              g->r_node_idx, (int)m, 0, bits_for(n), st));
-    k_fill_offsets32<<<scc_blocks(m + 1, 256, 148 * 64), 256, 0, st>>>(m, n, (const int32_t*)keys.p, g->r_begin);
-    SCC_CUDA(cudaPeekAtLastError());
+    SCC_CUDA(fill_offsets(m, n, (const int32_t*)keys.p, g->r_begin, st));
     return SCC_OK;
 }
 
@@ -350,11 +373,156 @@ extern "C" int scc_graph_upload_csr(scc_graph* g, const int32_t* begin, const in
     return SCC_OK;
 }
 
+// ------------------------------------------------------------------ pipelined upload
+// The forward CSR crosses the bus in UPLOAD_RUNS chunks of whole source lists;
+// each chunk's (destination, source) pairs are sorted by destination on a
+// second stream while the next chunk is in flight.  A chunk's sorted pairs
+// form a run; the stable sort keeps sources ascending inside a run and runs
+// are in source order, so an in-list is the concatenation of its segments in
+// the runs, in run order, which one scatter places.
+#define UPLOAD_RUNS 4
+#define UPLOAD_PIPELINE_MIN_EDGES (1LL << 22)
+
+struct RunBounds {
+    int64_t e[UPLOAD_RUNS + 1];      // edge range of each run
+};
+
+// r_begin[v] = sum over runs of the run-local offsets (edges with key < v)
+__global__ void k_runs_begin(int32_t n, const int32_t* __restrict__ off, int32_t* __restrict__ r_begin) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v <= n; v += (int64_t)gridDim.x * blockDim.x) {
+        int64_t t = 0;
+#pragma unroll
+        for (int j = 0; j < UPLOAD_RUNS; ++j) t += off[(int64_t)j * (n + 1) + v];
+        r_begin[v] = (int32_t)t;
+    }
+}
+
+// pos = r_begin[v] + (v's edges in earlier runs) + (rank inside this run's segment)
+__global__ void k_runs_scatter(int32_t n, RunBounds rb, const int32_t* __restrict__ keys,
+                               const int32_t* __restrict__ vals, const int32_t* __restrict__ off,
+                               const int32_t* __restrict__ r_begin, int32_t* __restrict__ out) {
+    const int64_t m = rb.e[UPLOAD_RUNS];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        int j = 0;
+        while (j + 1 < UPLOAD_RUNS && i >= rb.e[j + 1]) ++j;
+        const int32_t v = keys[i];
+        int64_t pos = (int64_t)__ldg(r_begin + v) + (i - rb.e[j]) - __ldg(off + (int64_t)j * (n + 1) + v);
+        for (int k = 0; k < j; ++k) {
+            const int32_t* o = off + (int64_t)k * (n + 1);
+            pos += __ldg(o + v + 1) - __ldg(o + v);
+        }
+        out[pos] = vals[i];
+    }
+}
+
+__global__ void k_expand_sources_range(int32_t s0, int32_t s1, const int32_t* __restrict__ begin,
+                                       int32_t* __restrict__ src) {
+    int lane = threadIdx.x & 31;
+    for (int64_t w = s0 + ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5); w < s1;
+         w += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int32_t b = begin[w], e = begin[w + 1];
+        for (int32_t k = b + lane; k < e; k += 32) src[k] = (int32_t)w;
+    }
+}
+
+namespace {
+struct Events {
+    cudaEvent_t ev[UPLOAD_RUNS + 1] = {};
+    cudaStream_t cs = nullptr;
+    ~Events() {
+        for (auto& e : ev) if (e) cudaEventDestroy(e);
+        if (cs) cudaStreamDestroy(cs);
+    }
+};
+// Declared after the scratch buffers, so it runs before their frees on the
+// caller's stream: that stream first waits for everything queued on the
+// helper stream, on the error paths too.
+struct JoinOnExit {
+    cudaStream_t st;
+    Events& evs;
+    ~JoinOnExit() {
+        if (evs.cs && evs.ev[UPLOAD_RUNS]) {
+            cudaEventRecord(evs.ev[UPLOAD_RUNS], evs.cs);
+            cudaStreamWaitEvent(st, evs.ev[UPLOAD_RUNS], 0);
+        }
+    }
+};
+}  // namespace
+
+static int upload_pipelined(scc_graph* g, const int32_t* begin, const int32_t* node_idx, cudaStream_t st) {
+    const int32_t n = g->n;
+    const int64_t m = g->m;
+    // run boundaries at whole source lists, about m / UPLOAD_RUNS edges each
+    RunBounds rb;
+    int32_t sv[UPLOAD_RUNS + 1];
+    sv[0] = 0;
+    sv[UPLOAD_RUNS] = n;
+    for (int j = 1; j < UPLOAD_RUNS; ++j) {
+        const int64_t target = m * j / UPLOAD_RUNS;
+        sv[j] = (int32_t)(std::lower_bound(begin, begin + n + 1, (int32_t)target) - begin);
+        if (sv[j] < sv[j - 1]) sv[j] = sv[j - 1];
+        if (sv[j] > n) sv[j] = n;
+    }
+    int64_t biggest = 0;
+    for (int j = 0; j <= UPLOAD_RUNS; ++j) rb.e[j] = begin[sv[j]];
+    for (int j = 0; j < UPLOAD_RUNS; ++j) biggest = std::max<int64_t>(biggest, rb.e[j + 1] - rb.e[j]);
+    SCC_REQUIRE(rb.e[UPLOAD_RUNS] == m && rb.e[0] == 0, SCC_ERR_INVALID, "CSR offsets do not run from 0 to m");
+
+    Events evs;
+    SCC_CUDA(cudaStreamCreateWithFlags(&evs.cs, cudaStreamNonBlocking));
+    for (auto& e : evs.ev) SCC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    AsyncScratch src(st), keys(st), vals(st), off(st), tmp(st);
+    JoinOnExit join{st, evs};
+    SCC_CUDA(src.alloc(sizeof(int32_t) * (size_t)m));
+    SCC_CUDA(keys.alloc(sizeof(int32_t) * (size_t)m));
+    SCC_CUDA(vals.alloc(sizeof(int32_t) * (size_t)m));
+    SCC_CUDA(off.alloc(sizeof(int32_t) * (size_t)UPLOAD_RUNS * ((size_t)n + 1)));
+    const int bits = bits_for(n);
+    size_t tb = 0;
+    SCC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, g->node_idx, (int32_t*)keys.p, (const int32_t*)src.p,
+                                             (int32_t*)vals.p, (int)biggest, 0, bits, evs.cs));
+    SCC_CUDA(tmp.alloc(tb));
+    SCC_CUDA(cudaMemcpyAsync(g->begin, begin, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, st));
+    for (int j = 0; j < UPLOAD_RUNS; ++j) {
+        const int64_t e0 = rb.e[j], c = rb.e[j + 1] - e0;
+        if (c > 0)
+            SCC_CUDA(cudaMemcpyAsync(g->node_idx + e0, node_idx + e0, sizeof(int32_t) * (size_t)c,
+                                     cudaMemcpyHostToDevice, st));
+        SCC_CUDA(cudaEventRecord(evs.ev[j], st));
+    }
+    int32_t* offp = (int32_t*)off.p;
+    for (int j = 0; j < UPLOAD_RUNS; ++j) {
+        const int64_t e0 = rb.e[j], c = rb.e[j + 1] - e0;
+        SCC_CUDA(cudaStreamWaitEvent(evs.cs, evs.ev[j], 0));
+        int32_t* oj = offp + (int64_t)j * (n + 1);
+        if (c == 0) {
+            SCC_CUDA(cudaMemsetAsync(oj, 0, sizeof(int32_t) * ((size_t)n + 1), evs.cs));
+            continue;
+        }
+        k_expand_sources_range<<<scc_blocks((int64_t)(sv[j + 1] - sv[j]) * 32, 256, 148 * 64), 256, 0, evs.cs>>>(
+            sv[j], sv[j + 1], g->begin, (int32_t*)src.p);
+        SCC_CUDA(cudaPeekAtLastError());
+        size_t tbj = tb;
+        SCC_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tbj, g->node_idx + e0, (int32_t*)keys.p + e0,
+                                                 (const int32_t*)src.p + e0, (int32_t*)vals.p + e0, (int)c, 0, bits,
+                                                 evs.cs));
+        SCC_CUDA(fill_offsets(c, n, (const int32_t*)keys.p + e0, oj, evs.cs));
+    }
+    k_runs_begin<<<scc_blocks((int64_t)n + 1, 256, 148 * 64), 256, 0, evs.cs>>>(n, offp, g->r_begin);
+    SCC_CUDA(cudaPeekAtLastError());
+    k_runs_scatter<<<scc_blocks(m, 256, 148 * 64), 256, 0, evs.cs>>>(n, rb, (const int32_t*)keys.p,
+                                                                     (const int32_t*)vals.p, offp, g->r_begin,
+                                                                     g->r_node_idx);
+    SCC_CUDA(cudaPeekAtLastError());
+    return SCC_OK;      // `join` makes the caller's stream resume after the transpose
+}
+
 extern "C" int scc_graph_upload_csr_out(scc_graph* g, const int32_t* begin, const int32_t* node_idx, void* stream) {
     SCC_REQUIRE(g && begin && (g->m == 0 || node_idx), SCC_ERR_INVALID, "NULL argument");
     SCC_CUDA(cudaSetDevice(g->device));
     cudaStream_t st = (cudaStream_t)stream;
     g->self_loops = -1;                      // new contents: count again when needed
+    if (g->m >= UPLOAD_PIPELINE_MIN_EDGES) return upload_pipelined(g, begin, node_idx, st);
     SCC_CUDA(cudaMemcpyAsync(g->begin, begin, sizeof(int32_t) * ((size_t)g->n + 1), cudaMemcpyHostToDevice, st));
     if (g->m > 0)
         SCC_CUDA(cudaMemcpyAsync(g->node_idx, node_idx, sizeof(int32_t) * (size_t)g->m, cudaMemcpyHostToDevice, st));

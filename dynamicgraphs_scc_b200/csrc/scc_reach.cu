@@ -550,6 +550,7 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
     double t0 = scc_trace_on() ? now_ms() : 0.0;
     while (qlen > 0) {
         const char* mode;
+        bool synced = false;      // the counters on the host already hold this step's results
         if (bottom_up) {
             SCC_TRY(scc_zero_counters(s, CTR_QLEN, 1));
             k_reach_bottomup<<<scc_blocks(a.live_count, REACH_THREADS, 148 * 16), REACH_THREADS, 0, s->stream>>>(a, qout);
@@ -636,11 +637,13 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
                 SCC_LAUNCHED(s);
                 k_reach_huge<<<148 * 8, REACH_THREADS, 0, s->stream>>>(a, s->hq, nhuge, s->hoff, qout);
                 SCC_LAUNCHED(s);
+            } else {
+                synced = true;
             }
             mode = nhuge > 0 ? "top-down+huge" : "top-down";
         }
         s->traversal_steps++;
-        SCC_TRY(scc_sync_counters(s));
+        if (!synced) SCC_TRY(scc_sync_counters(s));
         int32_t next = s->h_ctr[CTR_QLEN];
         if (bottom_up) {
             bottom_up = (int64_t)next * s->tune.bu_div > live2;
