@@ -111,12 +111,15 @@ int scc_read_edge_list(const char* path, int64_t capacity, int32_t* src, int32_t
  * (cudaStream_t as void*, NULL = legacy default stream). */
 int scc_graph_upload_csr(scc_graph* g, const int32_t* begin, const int32_t* node_idx,
                          const int32_t* r_begin, const int32_t* r_node_idx, void* stream);
-/* Re-upload only the forward CSR (host arrays of the graph's n and m) and
- * rebuild the transpose on the device -- a stable radix sort of (destination,
- * source) pairs, so in-lists come out sorted by source exactly as
- * make_reverse_edges (gm_graph/src/gm_graph.cc:193-287) leaves them.  Half the
- * host-to-device bytes of scc_graph_upload_csr; ordered on `stream`, whose
- * memory pool holds the sort's scratch until the stream reaches it. */
+/* Re-upload only the forward CSR (host arrays of the graph's n and m; begin
+ * must be a valid CSR offset array) and rebuild the transpose on the device --
+ * stable radix sorts of (destination, source) pairs, so in-lists come out
+ * sorted by source exactly as make_reverse_edges (gm_graph/src/gm_graph.cc:193-287)
+ * leaves them.  From 4 M edges the CSR crosses the bus in four chunks of whole
+ * source lists, each sorted on a helper stream while the next is in flight,
+ * then merged by one scatter.  Half the host-to-device bytes of
+ * scc_graph_upload_csr; ordered on `stream`, whose memory pool holds the
+ * scratch until the stream reaches it. */
 int scc_graph_upload_csr_out(scc_graph* g, const int32_t* begin, const int32_t* node_idx, void* stream);
 int scc_graph_free(scc_graph* g);                             /* graph_free() */
 int scc_graph_num_nodes(const scc_graph* g, int32_t* n);
