@@ -96,8 +96,7 @@ struct scc_state {
     int32_t* qb = nullptr;           // [2n+64] traversal queue B
     int32_t* aq = nullptr;           // [2n+64] asynchronous traversal queue, kept at -1 between uses
     int32_t* uf = nullptr;           // [n] union-find parents (weak-component split)
-    int32_t* cnt_out = nullptr;      // [n] live out-neighbour counts (counting peel on a fresh state)
-    int32_t* cnt_in = nullptr;       // [n] live in-neighbour counts
+    unsigned long long* cnt = nullptr;   // [n] live counts of the counting peel, (in << 32) | out; also n ints of scratch for updates
     int32_t* hq = nullptr;           // [2n+64] high-degree items deferred by a top-down level
     long long* hoff = nullptr;       // [2n+64] prefix of their degrees
     uint8_t* mark = nullptr;         // [n rounded to 4] reachability marks (bit0 FW, bit1 BW)
@@ -121,7 +120,7 @@ struct scc_state {
     // learned pivot (scc_mlp.cu)
     scc_pivot_model* pivot_model = nullptr;  // attached model (not owned)
     int pivot_mode = SCC_PIVOT_DEGREE;       // mode of the run in progress
-    bool cnt_valid = false;                  // cnt_out/cnt_in hold the first peel's residue
+    bool cnt_valid = false;                  // cnt holds the first peel's residue
     int32_t* pivot_cand = nullptr;           // [n] candidates of the learned choice (vertex ids)
     float* pivot_score = nullptr;            // [n] their scores
     void* pivot_x = nullptr;                 // [n] their BF16 feature rows (16 B each)

@@ -72,16 +72,17 @@ __device__ __forceinline__ float degree_log(const int32_t* __restrict__ off, int
     return lg1p((float)(__ldg(off + v + 1) - __ldg(off + v)));
 }
 
-__device__ void vertex_features(const RoundArgs& a, const int32_t* __restrict__ cnt_out,
-                                const int32_t* __restrict__ cnt_in, int32_t v, int32_t c, float* f) {
+__device__ void vertex_features(const RoundArgs& a, const unsigned long long* __restrict__ cnt, int32_t v,
+                                int32_t c, float* f) {
     int32_t ob = __ldg(a.begin + v), oe = __ldg(a.begin + v + 1);
     int32_t ib = __ldg(a.r_begin + v), ie = __ldg(a.r_begin + v + 1);
     float od = (float)(oe - ob), id = (float)(ie - ib);
     f[0] = lg1p(od);
     f[1] = lg1p(id);
     f[2] = lg1p(od * id);
-    f[3] = cnt_out ? lg1p((float)cnt_out[v]) : f[0];
-    f[4] = cnt_in ? lg1p((float)cnt_in[v]) : f[1];
+    const unsigned long long r = cnt ? cnt[v] : 0ull;        // peel residue, (in << 32) | out
+    f[3] = cnt ? lg1p((float)(uint32_t)r) : f[0];
+    f[4] = cnt ? lg1p((float)(uint32_t)(r >> 32)) : f[1];
     f[5] = lg1p((float)a.slot_count[c + 1]);
     float s = 0.f, mx = 0.f;
     int k = 0;
@@ -146,14 +147,14 @@ __device__ __forceinline__ uint4 pack_row(const float* f) {
 }
 
 // Training records: features of sampled vertices of the classes being pivoted.
-__global__ void k_pivot_log(RoundArgs a, const int32_t* __restrict__ cnt_out, const int32_t* __restrict__ cnt_in,
+__global__ void k_pivot_log(RoundArgs a, const unsigned long long* __restrict__ cnt,
                             LogArgs lg) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.live_count; i += (int64_t)gridDim.x * blockDim.x) {
         int32_t v = a.live[i];
         int32_t c = a.color[v];
         if (!traversed(a, c) || (pivot_hash((uint32_t)v ^ lg.salt) & 0xFFFFu) >= lg.thresh) continue;
         float f[MLP_IN];
-        vertex_features(a, cnt_out, cnt_in, v, c, f);
+        vertex_features(a, cnt, v, c, f);
         int32_t k = atomicAdd(lg.ctr, 1);
         if (k < lg.cap) {
 #pragma unroll
@@ -190,14 +191,14 @@ __global__ void k_pivot_candidates(RoundArgs a, int32_t* __restrict__ cand, int3
     }
 }
 
-__global__ void k_cand_features(RoundArgs a, const int32_t* __restrict__ cnt_out, const int32_t* __restrict__ cnt_in,
+__global__ void k_cand_features(RoundArgs a, const unsigned long long* __restrict__ cnt,
                                 const int32_t* __restrict__ cand, const int32_t* __restrict__ ncand,
                                 uint4* __restrict__ rows) {
     const int32_t k = *ncand;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < k; i += (int64_t)gridDim.x * blockDim.x) {
         int32_t v = cand[i];
         float f[MLP_IN];
-        vertex_features(a, cnt_out, cnt_in, v, a.color[v], f);
+        vertex_features(a, cnt, v, a.color[v], f);
         rows[i] = pack_row(f);
     }
 }
@@ -654,15 +655,14 @@ int scc_impl_pivot_prepare(const scc_graph* g, scc_state* s, RoundArgs& a, bool 
     unsigned blocks = scc_blocks(a.live_count);
     k_class_sizes<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
     SCC_LAUNCHED(s);
-    const int32_t* co = s->cnt_valid ? s->cnt_out : nullptr;
-    const int32_t* ci = s->cnt_valid ? s->cnt_in : nullptr;
+    const unsigned long long* cr = s->cnt_valid ? s->cnt : nullptr;
     if (logging) {
         LogArgs lg;
         lg.x = s->log_x; lg.v = s->log_v; lg.size = s->log_size; lg.ctr = s->log_ctr; lg.cap = s->log_cap;
         double p = (double)s->log_per_round / (double)a.live_count;
         lg.thresh = p >= 1.0 ? 0x10000u : (uint32_t)std::max(1.0, p * 65536.0);
         lg.salt = 0x9E3779B9u * (++s->log_salt);
-        k_pivot_log<<<blocks, SCC_THREADS, 0, s->stream>>>(a, co, ci, lg);
+        k_pivot_log<<<blocks, SCC_THREADS, 0, s->stream>>>(a, cr, lg);
         SCC_LAUNCHED(s);
     }
     if (!learned) return SCC_OK;
@@ -673,7 +673,7 @@ int scc_impl_pivot_prepare(const scc_graph* g, scc_state* s, RoundArgs& a, bool 
     SCC_TRY(scc_zero_counters(s, CTR_SPARE1, 1));
     k_pivot_candidates<<<blocks, SCC_THREADS, 0, s->stream>>>(a, s->pivot_cand, ncand);
     SCC_LAUNCHED(s);
-    k_cand_features<<<blocks, SCC_THREADS, 0, s->stream>>>(a, co, ci, s->pivot_cand, ncand, (uint4*)s->pivot_x);
+    k_cand_features<<<blocks, SCC_THREADS, 0, s->stream>>>(a, cr, s->pivot_cand, ncand, (uint4*)s->pivot_x);
     SCC_LAUNCHED(s);
     k_mlp_score_tc<<<tc_blocks(a.live_count), TC_ROWS, TC_SMEM, s->stream>>>(
         (const uint4*)s->pivot_x, a.live_count, ncand, m->w16, s->pivot_score, s->ctr + CTR_ERROR);

@@ -221,7 +221,7 @@ extern "C" int scc_state_free(scc_state* s) {
     if (!s) return SCC_OK;
     cudaSetDevice(s->device);
     cudaFree(s->color); cudaFree(s->scc); cudaFree(s->wcc); cudaFree(s->live); cudaFree(s->live_tmp);
-    cudaFree(s->qa); cudaFree(s->qb); cudaFree(s->aq); cudaFree(s->uf); cudaFree(s->hq); cudaFree(s->hoff); cudaFree(s->cnt_out); cudaFree(s->cnt_in); cudaFree(s->mark); cudaFree(s->aux); cudaFree(s->block_sums);
+    cudaFree(s->qa); cudaFree(s->qb); cudaFree(s->aq); cudaFree(s->uf); cudaFree(s->hq); cudaFree(s->hoff); cudaFree(s->cnt); cudaFree(s->mark); cudaFree(s->aux); cudaFree(s->block_sums);
     cudaFree(s->ctr);
     if (s->h_ctr) cudaFreeHost(s->h_ctr);
     cudaFree(s->slot_key); cudaFree(s->slot_pivot); cudaFree(s->slot_fw); cudaFree(s->slot_bw); cudaFree(s->slot_count);
@@ -256,8 +256,7 @@ extern "C" int scc_state_create(const scc_graph* g, scc_state** out) {
     if (e == cudaSuccess) e = cudaMalloc(&s->qb, qb);
     if (e == cudaSuccess) e = cudaMalloc(&s->aq, qb);
     if (e == cudaSuccess) e = cudaMalloc(&s->uf, nb);
-    if (e == cudaSuccess) e = cudaMalloc(&s->cnt_out, nb);
-    if (e == cudaSuccess) e = cudaMalloc(&s->cnt_in, nb);
+    if (e == cudaSuccess) e = cudaMalloc(&s->cnt, 2 * nb);
     if (e == cudaSuccess) e = cudaMalloc(&s->hq, qb);
     if (e == cudaSuccess) e = cudaMalloc(&s->hoff, sizeof(long long) * (size_t)(2 * n + 64));
     if (e == cudaSuccess) e = cudaMemset(s->aq, 0xFF, qb);

@@ -157,11 +157,18 @@ __global__ void k_trim1_fresh(TrimArgs a, int32_t n) {
 // ------------------------------------------------------------------ counting peel
 // On a fresh state every vertex is live and of colour -1, so v's live
 // out-neighbour count is its out-degree minus its self-loops (a contiguous run
-// in the sorted list), from the offsets alone.  Peeling then needs one atomic
-// decrement per edge of a trimmed vertex: whoever brings a count to zero
-// trims that vertex (the colour CAS makes it happen once) and continues the
-// chain from it.  Counts track the live counts exactly, so the result is the
-// same fixpoint as the scanning peel.
+// in the sorted list), from the offsets alone.  Both counts sit in one 64-bit
+// word, (in << 32) | out.  Peeling needs one atomic per edge of a trimmed
+// vertex: it decrements one half of the neighbour's word, and the atomic that
+// takes the word from "both halves non-zero" to "one half zero" is unique, so
+// whoever performs it trims that vertex with plain stores and continues the
+// chain from it.  A vertex with a zero count from the start (a seed) never
+// makes that transition: the count set-up marks it SEED and the sweep alone
+// trims it.  Counts track the live counts exactly (a half is decremented once
+// per edge to a trimmed neighbour, so it never borrows), and the result is
+// the same fixpoint as the scanning peel.
+#define SCC_COLOR_SEED (-3)
+
 __device__ __forceinline__ int32_t self_run(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                                             int32_t v) {
     int32_t b = __ldg(off + v), e = __ldg(off + v + 1);
@@ -178,7 +185,7 @@ __device__ __forceinline__ int32_t self_run(const int32_t* __restrict__ off, con
 // self-loops (graphs built without them skip the adjacency reads entirely).
 __global__ void k_count_init(const int32_t* __restrict__ begin, const int32_t* __restrict__ node_idx,
                              const int32_t* __restrict__ r_begin, const int32_t* __restrict__ r_node_idx, int32_t n,
-                             int has_self, int32_t* __restrict__ cnt_out, int32_t* __restrict__ cnt_in) {
+                             int has_self, unsigned long long* __restrict__ cnt, int32_t* __restrict__ color) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         int32_t v = (int32_t)i;
         int32_t co = __ldg(begin + v + 1) - __ldg(begin + v), ci = __ldg(r_begin + v + 1) - __ldg(r_begin + v);
@@ -186,8 +193,8 @@ __global__ void k_count_init(const int32_t* __restrict__ begin, const int32_t* _
             co -= self_run(begin, node_idx, v);
             ci -= self_run(r_begin, r_node_idx, v);
         }
-        cnt_out[v] = co;
-        cnt_in[v] = ci;
+        cnt[v] = ((unsigned long long)(uint32_t)ci << 32) | (uint32_t)co;
+        if (co == 0 || ci == 0) color[v] = SCC_COLOR_SEED;
     }
 }
 
@@ -214,26 +221,20 @@ static int count_self_loops(const scc_graph* g, scc_state* s) {
 
 struct CountArgs {
     const int32_t* begin; const int32_t* node_idx; const int32_t* r_begin; const int32_t* r_node_idx;
-    int32_t* color; int32_t* scc; int32_t* cnt_out; int32_t* cnt_in;
+    int32_t* color; int32_t* scc; unsigned long long* cnt;
     int32_t* ovf; int32_t* ctr;
 };
 
-__device__ __forceinline__ bool count_trim(const CountArgs& a, int32_t v) {
-    if (atomicCAS(a.color + v, SCC_COLOR_INIT, SCC_COLOR_DONE) != SCC_COLOR_INIT) return false;
-    a.scc[v] = v;
-    return true;
-}
-
 #define PEEL_Q 256          // per-warp queue of trimmed vertices awaiting expansion
+#define CNT_IN_ONE (1ull << 32)
 
 // Expand this warp's queued trimmed vertices, 32 at a time, with their edges
 // spread over the lanes (a warp prefix sum of the degrees; each lane finds the
 // vertex owning its edge by a binary search over the lanes): every trimmed x
-// decrements the live count of each neighbour -- out-neighbours lose an
-// in-neighbour, in-neighbours an out-neighbour -- so a warp issues 32
-// independent atomics per round trip.  A count reaching zero trims that
-// neighbour (the colour CAS makes it happen once), which joins the queue, or
-// the overflow list when the queue is full.
+// decrements a count of each neighbour -- out-neighbours lose an in-neighbour,
+// in-neighbours an out-neighbour -- so a warp issues 32 independent atomics
+// per round trip.  The atomic that zeroes the first half of a word trims that
+// neighbour, which joins the queue, or the overflow list when the queue is full.
 __device__ void peel_drain(const CountArgs& a, int32_t* wq, int32_t& qn, int32_t& cnt) {
     const int lane = threadIdx.x & 31;
     const unsigned full = 0xFFFFFFFFu;
@@ -270,11 +271,23 @@ __device__ void peel_drain(const CountArgs& a, int32_t* wq, int32_t& qn, int32_t
             int32_t nv = -1;
             if (j < total) {
                 if (k < ood) {
+                    // out-neighbour w loses an in-neighbour: high half
                     int32_t w = __ldg(a.node_idx + oob + k);
-                    if (w != ox && atomicSub(a.cnt_in + w, 1) == 1 && count_trim(a, w)) nv = w;
+                    if (w != ox) {
+                        unsigned long long old = atomicAdd(a.cnt + w, 0ull - CNT_IN_ONE);
+                        if ((old >> 32) == 1ull && (uint32_t)old != 0u) nv = w;
+                    }
                 } else {
+                    // in-neighbour u loses an out-neighbour: low half
                     int32_t u = __ldg(a.r_node_idx + oib + (k - ood));
-                    if (u != ox && atomicSub(a.cnt_out + u, 1) == 1 && count_trim(a, u)) nv = u;
+                    if (u != ox) {
+                        unsigned long long old = atomicAdd(a.cnt + u, 0ull - 1ull);
+                        if ((uint32_t)old == 1u && (old >> 32) != 0ull) nv = u;
+                    }
+                }
+                if (nv >= 0) {
+                    a.color[nv] = SCC_COLOR_DONE;
+                    a.scc[nv] = nv;
                 }
             }
             const unsigned bal = __ballot_sync(full, nv >= 0);
@@ -296,9 +309,9 @@ __device__ void peel_drain(const CountArgs& a, int32_t* wq, int32_t& qn, int32_t
     }
 }
 
-// Sweep (items == NULL): every vertex with a zero count is trimmed and
-// expanded.  List (items != NULL): expand trimmed vertices that overflowed a
-// queue.  Each warp drains its queue after every 32 vertices.
+// Sweep (items == NULL): every seed is trimmed and expanded.  List (items !=
+// NULL): expand trimmed vertices that overflowed a queue.  Each warp drains
+// its queue after every 32 vertices.
 __global__ void __launch_bounds__(SCC_THREADS) k_count_peel(CountArgs a, int32_t n, const int32_t* __restrict__ items) {
     __shared__ int32_t queues[SCC_THREADS / 32][PEEL_Q];
     const int lane = threadIdx.x & 31;
@@ -312,8 +325,11 @@ __global__ void __launch_bounds__(SCC_THREADS) k_count_peel(CountArgs a, int32_t
             if (items) {
                 x = items[i];
             } else {
+                // only the sweep writes a seed's colour, so a plain read decides
                 int32_t v = (int32_t)i;
-                if ((__ldcg(a.cnt_out + v) == 0 || __ldcg(a.cnt_in + v) == 0) && count_trim(a, v)) {
+                if (a.color[v] == SCC_COLOR_SEED) {
+                    a.color[v] = SCC_COLOR_DONE;
+                    a.scc[v] = v;
                     x = v;
                     cnt++;
                 }
@@ -332,13 +348,13 @@ static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     int32_t n = g->n;
     CountArgs a;
     a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin; a.r_node_idx = g->r_node_idx;
-    a.color = s->color; a.scc = s->scc; a.cnt_out = s->cnt_out; a.cnt_in = s->cnt_in;
+    a.color = s->color; a.scc = s->scc; a.cnt = s->cnt;
     a.ovf = s->qa; a.ctr = s->ctr;
     SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
     SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
     SCC_TRY(count_self_loops(g, s));
     k_count_init<<<scc_blocks(n), SCC_THREADS, 0, s->stream>>>(g->begin, g->node_idx, g->r_begin, g->r_node_idx, n,
-                                                               g->self_loops > 0 ? 1 : 0, s->cnt_out, s->cnt_in);
+                                                               g->self_loops > 0 ? 1 : 0, s->cnt, s->color);
     SCC_LAUNCHED(s);
     k_count_peel<<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, n, nullptr);
     SCC_LAUNCHED(s);
@@ -419,7 +435,7 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
     if (n_items <= 0) return SCC_OK;
     // snapshot colours (aux) so overflowed vertices keep their pre-trim colour
     bool fresh = s->fresh && !use_live;
-    if (fresh && s->cnt_in) return trim1_counting(g, s, trimmed);
+    if (fresh && s->cnt) return trim1_counting(g, s, trimmed);
     if (fresh) {
         // every colour is -1: the snapshot the overflow path reads is that constant
         k_fill_aux<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(n_items, s->aux, SCC_COLOR_INIT);

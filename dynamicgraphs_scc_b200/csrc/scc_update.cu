@@ -359,7 +359,8 @@ extern "C" int scc_update_batch(scc_graph* g, scc_state* s, int64_t n_ins, const
     SCC_CUDA(cudaEventRecord(s->ev[9], st));
 
     // 2. deletions: re-decompose the SCCs that lost an internal edge
-    int32_t* flag = s->cnt_out;   // scratch, n ints
+    int32_t* flag = reinterpret_cast<int32_t*>(s->cnt);   // scratch, n ints: the peel residue is gone
+    s->cnt_valid = false;
     if (n_del > 0) {
         k_upd_fill<<<scc_blocks(n), SCC_THREADS, 0, st>>>(n, flag, 0);
         SCC_LAUNCHED(s);
