@@ -52,10 +52,25 @@ __global__ void k_slot_reset(RoundArgs a, int reset_slots) {
         atomicAdd(reinterpret_cast<unsigned long long*>(a.ctr + CTR_LIVE_EDGES), deg);
 }
 
+// One class (the global step): its slots are the only ones to reset.
+__global__ void k_slot_reset_one(RoundArgs a, int32_t c) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.slot_key[c + 1] = 0ull;
+        a.slot_pivot[c + 1] = SCC_NIL_NODE;
+        a.slot_count[c + 1] = 0;
+    }
+}
+
 // Per-class maximum of the pivot keys.  A warp whose lanes all belong to one
-// class reduces its keys first and issues one atomic.
-__global__ void k_pivot_key(RoundArgs a) {
+// class reduces its keys first and issues one atomic.  The atomic that first
+// raises a class's slot from zero (keys are never zero) lists the class, so the
+// pivots are seeded from the list, not by another pass over the live vertices.
+// sum_degrees: also total the in+out degree of the traversed vertices (what
+// k_slot_reset does when the classes' slots need resetting first).
+__global__ void k_pivot_key(RoundArgs a, int32_t* __restrict__ class_list, int32_t* __restrict__ class_count,
+                            int sum_degrees) {
     const int lane = threadIdx.x & 31;
+    unsigned long long deg = 0;
     int64_t limit = (((int64_t)a.live_count + 31) / 32) * 32;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += (int64_t)gridDim.x * blockDim.x) {
         int32_t c = SCC_COLOR_DONE;
@@ -63,8 +78,16 @@ __global__ void k_pivot_key(RoundArgs a) {
         if (i < a.live_count) {
             int32_t v = a.live[i];
             c = a.color[v];
-            if (c == SCC_COLOR_DONE || (a.use_only && c != a.only_color)) c = SCC_COLOR_DONE;
-            else k = pivot_key(a.begin, a.r_begin, v);
+            if (c == SCC_COLOR_DONE || (a.use_only && c != a.only_color)) {
+                c = SCC_COLOR_DONE;
+            } else {
+                unsigned outd = (unsigned)(__ldg(a.begin + v + 1) - __ldg(a.begin + v));
+                unsigned ind = (unsigned)(__ldg(a.r_begin + v + 1) - __ldg(a.r_begin + v));
+                unsigned long long prod = (unsigned long long)outd * ind;
+                if (prod > 0xFFFFFFFEull) prod = 0xFFFFFFFEull;
+                k = ((prod + 1ull) << 32) | pivot_hash((uint32_t)v);
+                deg += outd + ind;
+            }
         }
         unsigned grp = __match_any_sync(0xFFFFFFFFu, c);
         if (grp == 0xFFFFFFFFu) {
@@ -74,16 +97,23 @@ __global__ void k_pivot_key(RoundArgs a) {
             }
             if (lane != 0) continue;
         }
-        if (c != SCC_COLOR_DONE && k > a.slot_key[c + 1]) atomicMax(a.slot_key + c + 1, k);
+        if (c != SCC_COLOR_DONE && k > a.slot_key[c + 1]) {
+            if (atomicMax(a.slot_key + c + 1, k) == 0ull) class_list[atomicAdd(class_count, 1)] = c;
+        }
+    }
+    if (sum_degrees) {
+        for (int o = 16; o > 0; o >>= 1) deg += __shfl_down_sync(0xFFFFFFFFu, deg, o);
+        if (lane == 0 && deg) atomicAdd(reinterpret_cast<unsigned long long*>(a.ctr + CTR_LIVE_EDGES), deg);
     }
 }
 
-__global__ void k_pivot_pick(RoundArgs a, int32_t* q) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.live_count; i += (int64_t)gridDim.x * blockDim.x) {
-        int32_t v = a.live[i];
-        int32_t c = a.color[v];
-        if (c == SCC_COLOR_DONE || (a.use_only && c != a.only_color)) continue;
-        if (pivot_key(a.begin, a.r_begin, v) == a.slot_key[c + 1]) seed_pivot(a, v, c, q);
+// Each listed class pivots on the vertex its best key names.
+__global__ void k_pivot_seed(RoundArgs a, const int32_t* __restrict__ class_list,
+                             const int32_t* __restrict__ class_count, int32_t* q) {
+    const int32_t nc = *class_count;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nc; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t c = class_list[i];
+        seed_pivot(a, pivot_unhash((uint32_t)a.slot_key[c + 1]), c, q);
     }
 }
 
@@ -155,18 +185,28 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
     SCC_TRY(scc_zero_counters(s, CTR_COUNT, 4));
     SCC_TRY(scc_zero_counters(s, CTR_NUM_CLASSES, 1));
     SCC_TRY(scc_zero_counters(s, CTR_LIVE_EDGES, 2));
-    k_slot_reset<<<blocks, SCC_THREADS, 0, s->stream>>>(a, forced_pivot < 0 ? 1 : 0);
+    // one class: reset its slots alone and total the degrees in the key pass
+    const bool one_class = a.use_only && forced_pivot < 0;
+    if (one_class) {
+        k_slot_reset_one<<<1, 32, 0, s->stream>>>(a, only_color);
+    } else {
+        k_slot_reset<<<blocks, SCC_THREADS, 0, s->stream>>>(a, forced_pivot < 0 ? 1 : 0);
+    }
     SCC_LAUNCHED(s);
     if (forced_pivot >= 0) {
         k_pivot_forced<<<1, 32, 0, s->stream>>>(a, forced_pivot, s->qa);
         SCC_LAUNCHED(s);
     } else {
-        k_pivot_key<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
+        // the class list lives in hq (free until the traversal), its length in CTR_SPARE4
+        int32_t* nclass = s->ctr + CTR_SPARE4;
+        SCC_TRY(scc_zero_counters(s, CTR_SPARE4, 1));
+        k_pivot_key<<<blocks, SCC_THREADS, 0, s->stream>>>(a, s->hq, nclass, one_class ? 1 : 0);
         SCC_LAUNCHED(s);
         const bool learned = s->pivot_mode == SCC_PIVOT_LEARNED && s->pivot_model;
         if (learned || s->log_cap > 0) SCC_TRY(scc_impl_pivot_prepare(g, s, a, learned, s->qa));
         if (!learned) {
-            k_pivot_pick<<<blocks, SCC_THREADS, 0, s->stream>>>(a, s->qa);
+            k_pivot_seed<<<scc_blocks(s->live_count, SCC_THREADS, 148 * 4), SCC_THREADS, 0, s->stream>>>(a, s->hq, nclass,
+                                                                                                     s->qa);
             SCC_LAUNCHED(s);
         }
     }
@@ -229,7 +269,8 @@ extern "C" int scc_choose_pivot_from_color(const scc_graph* g, scc_state* s, int
     unsigned long long zero = 0;
     SCC_CUDA(cudaMemcpyAsync(s->slot_key + color + 1, &zero, sizeof(zero), cudaMemcpyHostToDevice, s->stream));
     if (s->live_count > 0) {
-        k_pivot_key<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
+        SCC_TRY(scc_zero_counters(s, CTR_SPARE4, 1));     // the key pass lists the class in hq
+        k_pivot_key<<<blocks, SCC_THREADS, 0, s->stream>>>(a, s->hq, s->ctr + CTR_SPARE4, 0);
         SCC_LAUNCHED(s);
     }
     unsigned long long key = 0;

@@ -28,6 +28,16 @@ __device__ __forceinline__ uint32_t pivot_hash(uint32_t v) {
     return x;
 }
 
+// The hash is a bijection (odd multipliers and xor-shifts), so a class's best
+// key names its pivot: multiply by the inverses mod 2^32 and undo the shifts.
+__device__ __forceinline__ int32_t pivot_unhash(uint32_t x) {
+    x ^= (x >> 13) ^ (x >> 26);
+    x *= 0xA5CB9243u;            // 0x85EBCA6B^-1 mod 2^32
+    x ^= x >> 16;
+    x *= 0x0E8B2F51u;            // 0x9E3779B1^-1 mod 2^32
+    return (int32_t)x;
+}
+
 // Pivot key: (min(in*out, 2^32-2)+1) << 32 | hash(v); never 0, unique per vertex.
 __device__ __forceinline__ unsigned long long pivot_key(const int32_t* __restrict__ begin,
                                                         const int32_t* __restrict__ r_begin, int32_t v) {
