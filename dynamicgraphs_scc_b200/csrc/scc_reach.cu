@@ -230,13 +230,35 @@ __global__ void __launch_bounds__(REACH_THREADS) k_reach_huge(RoundArgs a, const
 }
 
 // ------------------------------------------------------------------ bottom-up mode
+// True if a neighbour of v carries `bit` in its mark and belongs to v's class.
+// Four neighbours at a time: their adjacency entries, then their marks, are
+// loaded together, so a long scan costs two round trips per four.  A round
+// over one class (use_only) traverses only that class, so a marked neighbour
+// is of colour c and its colour need not be read; with several classes a
+// mark may come from another class's traversal.
+__device__ __forceinline__ bool parent_ok(const RoundArgs& a, int32_t u, int32_t c) {
+    return a.use_only || __ldg(a.color + u) == c;
+}
+
 __device__ __forceinline__ bool has_marked_parent(const RoundArgs& a, const int32_t* __restrict__ off,
                                                   const int32_t* __restrict__ adj, int32_t v, int32_t c,
                                                   unsigned bit) {
     int32_t b = __ldg(off + v), e = __ldg(off + v + 1);
-    for (int32_t k = b; k < e; ++k) {
+    int32_t k = b;
+    for (; k + 4 <= e; k += 4) {
+        int32_t u[4];
+        unsigned m[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) u[j] = __ldg(adj + k + j);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) m[j] = *(volatile uint8_t*)(a.mark + u[j]);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if ((m[j] & bit) && parent_ok(a, u[j], c)) return true;
+    }
+    for (; k < e; ++k) {
         int32_t u = __ldg(adj + k);
-        if ((*(volatile uint8_t*)(a.mark + u) & bit) && __ldg(a.color + u) == c) return true;
+        if ((*(volatile uint8_t*)(a.mark + u) & bit) && parent_ok(a, u, c)) return true;
     }
     return false;
 }
