@@ -171,12 +171,15 @@ static RoundArgs round_args(const scc_graph* g, scc_state* s) {
 // One FW-BW round over every live class (only_color == INT32_MIN) or one class.
 // Requires the live list.  *scc_found = vertices finished, *active = classes pivoted.
 int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int32_t forced_pivot,
-                      int32_t* scc_found, int32_t* active) {
+                      int32_t* scc_found, int32_t* active, bool pipeline) {
     *scc_found = 0;
     if (active) *active = 0;
     s->fresh = false;
     if (s->live_count <= 0) return SCC_OK;
-    SCC_TRY(scc_sync_counters(s));
+    // inside the pipeline the host counters are current here (the last step
+    // synchronised them or set the colour counter itself); from the phase API
+    // they are read again
+    if (!pipeline) SCC_TRY(scc_sync_counters(s));
     SCC_TRY(scc_impl_ensure_colour_cap(s, (int64_t)s->h_ctr[CTR_NEXT_COLOR] + 2LL * s->live_count + 1024));
     RoundArgs a = round_args(g, s);
     a.use_only = (only_color != INT32_MIN);
@@ -218,6 +221,11 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
     SCC_TRY(scc_zero_counters(s, CTR_COUNT, 3));
     k_classify<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
     SCC_LAUNCHED(s);
+    if (pipeline) {
+        // the caller's compaction synchronises next; it leaves CTR_COUNT alone
+        *scc_found = -1;
+        return SCC_OK;
+    }
     SCC_TRY(scc_sync_counters(s));
     *scc_found = s->h_ctr[CTR_COUNT];
     return SCC_OK;
@@ -241,8 +249,9 @@ int scc_impl_resolve_all(const scc_graph* g, scc_state* s, bool classes_split) {
         else SCC_TRY(scc_impl_uf_split(g, s, &classes));
         int32_t live_before = s->live_count;
         int32_t found = 0, act = 0;
-        SCC_TRY(scc_impl_fb_round(g, s, INT32_MIN, -1, &found, &act));
-        SCC_TRY(scc_impl_compact_live(g, s, false));
+        SCC_TRY(scc_impl_fb_round(g, s, INT32_MIN, -1, &found, &act, true));
+        SCC_TRY(scc_impl_compact_live(g, s, false));   // synchronises: classify's count is current
+        found = s->h_ctr[CTR_COUNT];
         if (scc_trace_on())
             fprintf(stderr, "[scc] round %d: trimmed=%d live=%d classes=%d scc_found=%d left=%d\n", round, t,
                     live_before, classes, found, s->live_count);

@@ -167,7 +167,7 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
 int scc_impl_trim2(const scc_graph* g, scc_state* s, int32_t* trimmed);
 int scc_impl_ensure_colour_cap(scc_state* s, int64_t need);
 int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int32_t forced_pivot,
-                      int32_t* scc_found, int32_t* active_classes);
+                      int32_t* scc_found, int32_t* active_classes, bool pipeline = false);
 int scc_impl_wcc(const scc_graph* g, scc_state* s);
 int scc_impl_uf_split(const scc_graph* g, scc_state* s, int32_t* num_classes);
 bool scc_trace_on();

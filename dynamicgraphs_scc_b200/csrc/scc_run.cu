@@ -96,11 +96,11 @@ static int run_method(const scc_graph* g, scc_state* s, int method, scc_run_stat
     }
     // GLOBAL_BFS: do_fw_bw_global_main(G, -1, count, false)
     int32_t found = 0, act = 0;
-    SCC_TRY(scc_impl_fb_round(g, s, SCC_COLOR_INIT, -1, &found, &act));
-    st->first_scc_size = found;
+    SCC_TRY(scc_impl_fb_round(g, s, SCC_COLOR_INIT, -1, &found, &act, true));
     SCC_TRY(record(s, 2));
     // TRIM1 (+ TRIM2 + TRIM1 for method 2, scc_main.cc:410-423)
-    SCC_TRY(scc_impl_compact_live(g, s, false));
+    SCC_TRY(scc_impl_compact_live(g, s, false));   // synchronises: classify's count is current
+    st->first_scc_size = s->h_ctr[CTR_COUNT];
     int32_t t2 = 0;
     SCC_TRY(scc_impl_trim1(g, s, true, &t));
     t2 += t;

@@ -281,6 +281,7 @@ int scc_impl_uf_split(const scc_graph* g, scc_state* s, int32_t* num_classes) {
     int32_t k = s->h_ctr[CTR_NUM_CLASSES];
     int32_t last = k - 1;
     SCC_CUDA(cudaMemcpyAsync(s->ctr + CTR_NEXT_COLOR, &last, sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
+    s->h_ctr[CTR_NEXT_COLOR] = last;     // the host mirror stays current for the next round
     *num_classes = k;
     return SCC_OK;
 }
