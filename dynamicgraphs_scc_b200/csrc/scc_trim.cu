@@ -23,13 +23,22 @@
 
 __device__ __forceinline__ int32_t ld_cg(const int32_t* p) { return __ldcg(p); }
 
-// true if v has a neighbour w != v of colour c in (off, adj)
+// true if v has a neighbour w != v of colour c in (off, adj).  Four entries
+// at a time: their adjacency loads, then their colour loads, are issued
+// together (short lists included), so a scan costs two round trips per four
+// neighbours; every colour read still follows the caller's fence.
 __device__ __forceinline__ bool has_live_nbr(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                                              const int32_t* color, int32_t v, int32_t c) {
     int32_t b = __ldg(off + v), e = __ldg(off + v + 1);
-    for (int32_t k = b; k < e; ++k) {
-        int32_t w = __ldg(adj + k);
-        if (w != v && ld_cg(color + w) == c) return true;
+    for (int32_t k = b; k < e; k += 4) {
+        int32_t w[4], col[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) w[j] = (k + j < e) ? __ldg(adj + k + j) : v;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) col[j] = (w[j] != v) ? ld_cg(color + w[j]) : SCC_COLOR_DONE;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (w[j] != v && col[j] == c) return true;
     }
     return false;
 }
