@@ -234,9 +234,16 @@ __global__ void k_uf_hook(const int32_t* __restrict__ begin, const int32_t* __re
             }
         }
         if (deg <= 32) {
-            for (int32_t k = b; k < e; ++k) {
-                int32_t w = __ldg(node_idx + k);
-                if (w != v && __ldg(color + w) == c) uf_union(uf, v, w);
+            // four neighbours' adjacency entries, then their colours, loaded together
+            for (int32_t k = b; k < e; k += 4) {
+                int32_t w[4], col[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) w[j] = (k + j < e) ? __ldg(node_idx + k + j) : v;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) col[j] = (w[j] != v) ? __ldg(color + w[j]) : SCC_COLOR_DONE;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (w[j] != v && col[j] == c) uf_union(uf, v, w[j]);
             }
         }
     }
