@@ -1,6 +1,6 @@
 """GPU: failure paths, injected on the host (no test faults, traps or hangs the
-GPU).  An allocation that fails inside an update returns SCC_ERR_OOM and leaves
-the graph as it was; a bounded device wait that runs out (the drain is handed a
+GPU).  An allocation that fails inside an update or a pipelined CSR upload
+returns SCC_ERR_OOM and leaves the graph as it was; a bounded device wait that runs out (the drain is handed a
 queue slot nobody fills) returns SCC_ERR_TIMEOUT, and the state decomposes
 correctly again after a reset."""
 import numpy as np
@@ -61,4 +61,33 @@ def test_drain_wait_limit_reports_timeout_and_recovers(gpu):
     st.reset()
     st.run(2)
     assert np.array_equal(st.canonical_labels(), O.tarjan_canonical(csr[0], csr[1]))
+    st.free(); g.free()
+
+
+@pytest.mark.parametrize("countdown", [1, 3, 5])
+def test_pipelined_upload_allocation_failure(gpu, countdown):
+    # above 4 M edges the CSR-only upload sorts chunks on a helper stream; an
+    # allocation failing at any of its five scratch buffers returns SCC_ERR_OOM
+    # before any copy, leaves the graph as it was, and a retry is exact
+    n = 800000
+    s1, d1 = random_graph(n, 5000000, 41)
+    s2, d2 = random_graph(n, 5000000, 42)
+    csr1, csr2 = O.build_csr(n, s1, d1), O.build_csr(n, s2, d2)
+    g = Graph.from_edges(n, s1, d1)
+    capi.call("scc_debug_inject", SCC_INJECT_ALLOC, countdown)
+    try:
+        with pytest.raises(SccError) as ei:
+            g.upload_csr(csr2[0], csr2[1])
+        assert ei.value.status == SCC_ERR_OOM
+    finally:
+        capi.call("scc_debug_inject", SCC_INJECT_ALLOC, 0)
+    for got, exp in zip(g.csr(), csr1):
+        assert np.array_equal(got, exp)
+    g.upload_csr(csr2[0], csr2[1])
+    st = State(g)
+    st.synchronize()
+    for got, exp in zip(g.csr(), csr2):
+        assert np.array_equal(got, exp)
+    st.run(2)
+    assert np.array_equal(st.canonical_labels(), O.tarjan_canonical(csr2[0], csr2[1]))
     st.free(); g.free()
