@@ -330,13 +330,130 @@ def bench_serving(args, local_rank):
     print(json.dumps(line))
 
 
+LEVELS = dict(rmat_scale=24, edge_factor=16, grid_side=4096, seed=2024)          # C2's graph
+LEVELS_SAMPLE = dict(rmat_scale=18, edge_factor=16, grid_side=512, seed=2024)     # the reference's sample
+LEVELS_BATCH = 100                                                                # inserted edges per batch
+
+
+def scc_list_ids(labels):
+    """scc_list.txt ids of canonical labels: ascending smallest member is the
+    order of first appearance over the vertices."""
+    _, ids = np.unique(labels, return_inverse=True)
+    return ids.astype(np.int32), int(ids.max()) + 1 if ids.size else 0
+
+
+def bench_levels(args, local_rank):
+    """Method 7's preprocessing (create_scc_edges with met_algo 7,
+    src/common_main.h:180-262) on C2's decomposition: the condensation DAG of
+    the old labels, its topological levels, the levels a batch affects, and the
+    condensation with the batch; then the trim shortcut and the run on it.  The
+    entry points take and return host arrays, as the reference's vectors, and
+    synchronise: host wall clock around each call."""
+    import torch
+    from dynamicgraphs_scc_b200 import Graph, State, affected_levels, condensation_graph, topological_levels
+    torch.cuda.set_device(local_rank)
+    g = Graph.generate(**LEVELS, device=local_rank)
+    n, m = g.num_nodes(), g.num_edges()
+    st = State(g)
+    st.run(2)
+    ids, k = scc_list_ids(st.canonical_labels())
+    rng = np.random.default_rng(7)
+    isrc = rng.integers(0, n, LEVELS_BATCH).astype(np.int32)
+    idst = rng.integers(0, n, LEVELS_BATCH).astype(np.int32)
+
+    def bundle():
+        t = [time.perf_counter()]
+        dag = condensation_graph(g, ids, k)
+        t.append(time.perf_counter())
+        lev, ml = topological_levels(dag)
+        t.append(time.perf_counter())
+        aff, z = affected_levels(dag, lev, ml, ids, isrc, idst)
+        t.append(time.perf_counter())
+        cond = condensation_graph(g, ids, k, isrc, idst)
+        t.append(time.perf_counter())
+        md = dag.num_edges()
+        dag.free()
+        return cond, lev, ml, aff, z, md, [1e3 * (b - a) for a, b in zip(t, t[1:])]
+
+    for _ in range(args.warmup):
+        cond, *_ = bundle()
+        cond.free()
+    parts = []
+    for _ in range(args.steps):
+        cond, lev, ml, aff, z, md, p = bundle()
+        parts.append(p)
+        cond.free()
+    part_ms = [statistics.mean(x) for x in zip(*parts)]
+    total_ms = sum(part_ms)
+    # the trim shortcut and the run over the condensation with the batch
+    cond, lev, ml, aff, z, md, _ = bundle()
+    cs = State(cond)
+    run_ms = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        cs.reset()
+        fin = cs.finish_unaffected(lev, aff, ml)
+        r = cs.run(2)
+        if i >= args.warmup:
+            run_ms.append(1e3 * (time.perf_counter() - t0))
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = levels_reference()
+    line = {
+        "metric": "method-7 preprocessing (condensation, topological levels, affected levels, batch condensation)",
+        "value": round(m / (total_ms * 1e-3) / 1e9, 4), "unit": "Gedges/s (original edges)", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
+        "timing": "host wall clock around synchronous entry points (host arrays in and out)",
+        "parts_ms": {"condensation": round(part_ms[0], 3), "topological_levels": round(part_ms[1], 3),
+                     "affected_levels": round(part_ms[2], 3), "batch_condensation": round(part_ms[3], 3)},
+        "shortcut_and_run_ms": round(statistics.mean(run_ms), 3),
+        "config": {"workload": "C2 (R-MAT s24 ef16 U 4096x4096 oriented grid) decomposed, then method 7 on its "
+                               f"condensation with a {LEVELS_BATCH}-edge batch",
+                   "n": n, "m": m, "sccs": k, "condensation_edges": md, "max_level": ml,
+                   "unaffected_levels": z, "finished_by_shortcut": fin, "sccs_after": r["num_sccs"]},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+def levels_reference():
+    """The reference's own create_scc_edges (met_algo 7; one OpenMP thread, as
+    its unlocked push_backs require) on a sample of the same shape, through the
+    oracle's build of the reference."""
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from oracle import oracle as O
+    from dynamicgraphs_scc_b200 import generate_edges_host
+    if not O.ref_available():
+        return {"value": None, "unit": "Gedges/s", "cores": 1, "kind": "reference",
+                "sample": "reference library not built"}
+    n, s, d = generate_edges_host(**LEVELS_SAMPLE)
+    s, d = O.dedup_edges(s, d, drop_self_loops=True, n=n)
+    csr = O.build_csr(n, s, d)
+    ids, k = scc_list_ids(O.tarjan_canonical(csr[0], csr[1]))
+    rng = np.random.default_rng(7)
+    isrc = rng.integers(0, n, LEVELS_BATCH).astype(np.int32)
+    idst = rng.integers(0, n, LEVELS_BATCH).astype(np.int32)
+    b, a = O.condensation_csr(ids, k, s, d)
+    lev, ml = O.topo_levels(b, a)
+    _, z = O.affected_levels(ids, lev, ml, isrc, idst)
+    if z == 0:      # its closing loop runs past the end when no level is left unaffected
+        return {"value": None, "unit": "Gedges/s", "cores": 1, "kind": "reference",
+                "sample": "batch leaves no level unaffected"}
+    t0 = time.perf_counter()
+    O.ref_method7_levels(n, s, d, isrc, idst, ids, k)
+    ms = 1e3 * (time.perf_counter() - t0)
+    return {"value": round(s.size / (ms * 1e-3) / 1e9, 5), "unit": "Gedges/s", "cores": 1, "kind": "reference",
+            "sample": f"{LEVELS_SAMPLE} n={n} m={s.size}: {ms:.1f} ms"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5", "levels"])
     ap.add_argument("--tune-trials", type=int, default=8)
     ap.add_argument("--batches", type=int, default=200)
     ap.add_argument("--coalesce", type=int, default=1, help="c5: queued batches of a session composed per update")
@@ -356,6 +473,18 @@ def main():
             return
         if rank == 0:
             bench_serving(args, local_rank)
+        return
+
+    if args.workload == "levels":
+        if rank == 0:
+            if args.impl == "reference":
+                cpu = levels_reference()
+                print(json.dumps({"impl": "reference", "metric": "method-7 preprocessing (create_scc_edges)",
+                                  "value": cpu["value"], "unit": cpu["unit"], "cpu_baseline": cpu,
+                                  "e2e": {"value": cpu["value"], "unit": cpu["unit"], "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0}}))
+            else:
+                bench_levels(args, local_rank)
         return
 
     if args.workload == "c4":

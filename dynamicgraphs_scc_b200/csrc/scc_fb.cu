@@ -22,8 +22,16 @@
 // of the traversal compares frontier edges against it).  Lanes of a warp that
 // share a class reset its slots once, and a thread skips the class it reset
 // last, so a round over one huge class does not pile stores onto one address.
+// Also the largest single degree (a hub keeps a round out of the
+// asynchronous drain, whose warps would each expand it alone).
+__device__ __forceinline__ void max_degree_add(int32_t* dst, unsigned d) {
+    for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_down_sync(0xFFFFFFFFu, d, o));
+    if ((threadIdx.x & 31) == 0 && d) atomicMax(dst, (int32_t)min(d, 0x7FFFFFFFu));
+}
+
 __global__ void k_slot_reset(RoundArgs a, int reset_slots) {
     unsigned long long deg = 0;
+    unsigned dmax = 0;
     int32_t last = INT32_MIN;
     const int lane = threadIdx.x & 31;
     int64_t limit = (((int64_t)a.live_count + 31) / 32) * 32;
@@ -32,11 +40,14 @@ __global__ void k_slot_reset(RoundArgs a, int reset_slots) {
         if (i < a.live_count) {
             int32_t v = a.live[i];
             c = a.color[v];
-            if (c != SCC_COLOR_DONE && !(a.use_only && c != a.only_color))
-                deg += (unsigned)(__ldg(a.begin + v + 1) - __ldg(a.begin + v)) +
-                       (unsigned)(__ldg(a.r_begin + v + 1) - __ldg(a.r_begin + v));
-            else
+            if (c != SCC_COLOR_DONE && !(a.use_only && c != a.only_color)) {
+                unsigned dv = (unsigned)(__ldg(a.begin + v + 1) - __ldg(a.begin + v)) +
+                              (unsigned)(__ldg(a.r_begin + v + 1) - __ldg(a.r_begin + v));
+                deg += dv;
+                dmax = max(dmax, dv);
+            } else {
                 c = SCC_COLOR_DONE;
+            }
         }
         if (!reset_slots) continue;
         unsigned grp = __match_any_sync(0xFFFFFFFFu, c);
@@ -50,6 +61,7 @@ __global__ void k_slot_reset(RoundArgs a, int reset_slots) {
     for (int o = 16; o > 0; o >>= 1) deg += __shfl_down_sync(0xFFFFFFFFu, deg, o);
     if ((threadIdx.x & 31) == 0 && deg)
         atomicAdd(reinterpret_cast<unsigned long long*>(a.ctr + CTR_LIVE_EDGES), deg);
+    max_degree_add(a.ctr + CTR_MAXDEG, dmax);
 }
 
 // One class (the global step): its slots are the only ones to reset.
@@ -71,6 +83,7 @@ __global__ void k_pivot_key(RoundArgs a, int32_t* __restrict__ class_list, int32
                             int sum_degrees) {
     const int lane = threadIdx.x & 31;
     unsigned long long deg = 0;
+    unsigned dmax = 0;
     int64_t limit = (((int64_t)a.live_count + 31) / 32) * 32;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < limit; i += (int64_t)gridDim.x * blockDim.x) {
         int32_t c = SCC_COLOR_DONE;
@@ -87,6 +100,7 @@ __global__ void k_pivot_key(RoundArgs a, int32_t* __restrict__ class_list, int32
                 if (prod > 0xFFFFFFFEull) prod = 0xFFFFFFFEull;
                 k = ((prod + 1ull) << 32) | pivot_hash((uint32_t)v);
                 deg += outd + ind;
+                dmax = max(dmax, outd + ind);
             }
         }
         unsigned grp = __match_any_sync(0xFFFFFFFFu, c);
@@ -104,6 +118,7 @@ __global__ void k_pivot_key(RoundArgs a, int32_t* __restrict__ class_list, int32
     if (sum_degrees) {
         for (int o = 16; o > 0; o >>= 1) deg += __shfl_down_sync(0xFFFFFFFFu, deg, o);
         if (lane == 0 && deg) atomicAdd(reinterpret_cast<unsigned long long*>(a.ctr + CTR_LIVE_EDGES), deg);
+        max_degree_add(a.ctr + CTR_MAXDEG, dmax);
     }
 }
 
@@ -175,6 +190,7 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
     *scc_found = 0;
     if (active) *active = 0;
     s->fresh = false;
+    s->prefinished = false;
     if (s->live_count <= 0) return SCC_OK;
     // inside the pipeline the host counters are current here (the last step
     // synchronised them or set the colour counter itself); from the phase API
@@ -188,6 +204,7 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
     SCC_TRY(scc_zero_counters(s, CTR_COUNT, 4));
     SCC_TRY(scc_zero_counters(s, CTR_NUM_CLASSES, 1));
     SCC_TRY(scc_zero_counters(s, CTR_LIVE_EDGES, 2));
+    SCC_TRY(scc_zero_counters(s, CTR_MAXDEG, 1));
     // one class: reset its slots alone and total the degrees in the key pass
     const bool one_class = a.use_only && forced_pivot < 0;
     if (one_class) {

@@ -65,6 +65,7 @@ enum {
     CTR_LIVE_EDGES = 18, // u64 (slots 18-19): in+out degree of the vertices being traversed
     CTR_ASYNC_ITEMS = 20,// u64 (slots 20-21): items expanded by the asynchronous drain (ledger)
     CTR_ASYNC_EDGES = 22,// u64 (slots 22-23): edges scanned by it
+    CTR_MAXDEG = 24,     // largest in+out degree among the vertices a round traverses
     // asynchronous traversal queue counters, one 128-byte line each (polled by idle warps)
     CTR_AHEAD = 32,
     CTR_ATAIL = 64,
@@ -85,6 +86,7 @@ struct scc_state {
     int64_t traversal_steps = 0;
     int32_t fb_rounds = 0;           // recursion rounds (statistics)
     bool fresh = false;              // colours all -1 and nothing finished (set by reset, cleared by any phase)
+    bool prefinished = false;        // fresh except vertices finished as their own SCC (method 7's shortcut)
 
     int32_t* color = nullptr;        // G_Color [n]
     int32_t* scc = nullptr;          // G_SCC   [n]

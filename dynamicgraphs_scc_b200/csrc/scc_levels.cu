@@ -19,11 +19,21 @@
 #include "scc_internal.cuh"
 
 #define LEVEL_Q 256          // per-warp queue of released nodes awaiting expansion
+#define LEVEL_HUB 4096       // a released node with more out-edges is expanded over the whole grid
 
 struct LevelArgs {
     const int32_t* begin; const int32_t* node_idx; const int32_t* r_begin;
     int32_t* cnt; int32_t* level; int32_t* ovf; int32_t* ovf_count;
+    int32_t* hub; int32_t* hub_count;      // released hubs set aside for k_level_hub
 };
+
+// One out-edge of released x (whose level is lx - 1): raise the child's level,
+// then take its in-count; returns the child if this released it, else -1.
+__device__ __forceinline__ int32_t level_edge(const LevelArgs& a, int32_t w, int32_t lx) {
+    atomicMax(a.level + w, lx);
+    __threadfence();
+    return atomicSub(a.cnt + w, 1) == 1 ? w : -1;
+}
 
 __global__ void k_level_init(int32_t n, const int32_t* __restrict__ r_begin, int32_t* __restrict__ cnt,
                              int32_t* __restrict__ level) {
@@ -51,6 +61,10 @@ __device__ void level_drain(const LevelArgs& a, int32_t* wq, int32_t& qn) {
             ob = __ldg(a.begin + x);
             od = __ldg(a.begin + x + 1) - ob;
             lx = __ldcg(a.level + x) + 1;
+            if (od > LEVEL_HUB) {          // too many edges for one warp: the host expands it
+                a.hub[atomicAdd(a.hub_count, 1)] = x;
+                od = 0;
+            }
         }
         int32_t incl = od;
         for (int o = 1; o < 32; o <<= 1) {
@@ -71,12 +85,7 @@ __device__ void level_drain(const LevelArgs& a, int32_t* wq, int32_t& qn) {
             const int32_t oob = __shfl_sync(full, ob, owner);
             const int32_t olx = __shfl_sync(full, lx, owner);
             int32_t nv = -1;
-            if (j < total) {
-                int32_t w = __ldg(a.node_idx + oob + k);
-                atomicMax(a.level + w, olx);
-                __threadfence();
-                if (atomicSub(a.cnt + w, 1) == 1) nv = w;
-            }
+            if (j < total) nv = level_edge(a, __ldg(a.node_idx + oob + k), olx);
             const unsigned bal = __ballot_sync(full, nv >= 0);
             if (bal) {
                 const int32_t r = __popc(bal & ((1u << lane) - 1u)), nn = __popc(bal);
@@ -119,6 +128,57 @@ __global__ void __launch_bounds__(SCC_THREADS) k_level_peel(LevelArgs a, int32_t
     }
 }
 
+// Inclusive prefix of the hubs' out-degrees (one block; hoff[j] = end of hub j).
+__global__ void k_level_hub_prefix(const int32_t* __restrict__ begin, const int32_t* __restrict__ hubs, int32_t cnt,
+                                   long long* __restrict__ hoff) {
+    __shared__ long long part[1024];
+    int t = threadIdx.x;
+    int32_t per = (cnt + 1023) / 1024;
+    int32_t b = t * per, e = min(cnt, b + per);
+    long long sum = 0;
+    for (int32_t j = b; j < e; ++j) sum += __ldg(begin + hubs[j] + 1) - __ldg(begin + hubs[j]);
+    part[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        long long v = (t >= o) ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    long long run = (t == 0) ? 0 : part[t - 1];
+    for (int32_t j = b; j < e; ++j) {
+        run += __ldg(begin + hubs[j] + 1) - __ldg(begin + hubs[j]);
+        hoff[j] = run;
+    }
+}
+
+// Edge-parallel expansion of released hubs: thread t takes edge t of their
+// concatenated out-lists; the children it releases join the overflow list.
+__global__ void k_level_hub(LevelArgs a, const int32_t* __restrict__ hubs, int32_t cnt,
+                            const long long* __restrict__ hoff) {
+    const long long total = hoff[cnt - 1];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long limit = ((total + 31) / 32) * 32;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < limit; t += stride) {
+        int32_t nv = -1;
+        if (t < total) {
+            int32_t lo = 0, hi = cnt - 1;
+            while (lo < hi) { int32_t mid = (lo + hi) >> 1; if (hoff[mid] > t) hi = mid; else lo = mid + 1; }
+            const int32_t x = hubs[lo];
+            const long long start = lo ? hoff[lo - 1] : 0;
+            nv = level_edge(a, __ldg(a.node_idx + __ldg(a.begin + x) + (t - start)), __ldcg(a.level + x) + 1);
+        }
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, nv >= 0);
+        if (bal) {
+            const int lane = threadIdx.x & 31;
+            int32_t base = 0;
+            if (lane == 0) base = atomicAdd(a.ovf_count, __popc(bal));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (nv >= 0) a.ovf[base + __popc(bal & ((1u << lane) - 1u))] = nv;
+        }
+    }
+}
+
 __global__ void k_level_max(int32_t n, const int32_t* __restrict__ level, int32_t* __restrict__ out) {
     int32_t m = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -150,29 +210,48 @@ static int levels_on_device(const scc_graph* g, cudaStream_t st, int32_t* d_leve
     int32_t n = g->n;
     *max_level = 0;
     if (n == 0) return SCC_OK;
-    Buf cnt, ovf, list, ctr;
+    Buf cnt, ovf, list, ctr, hub, hubs, hoff;
     SCC_TRY(get(cnt, sizeof(int32_t) * (size_t)n, st));
     SCC_TRY(get(ovf, sizeof(int32_t) * (size_t)n, st));
     SCC_TRY(get(list, sizeof(int32_t) * (size_t)n, st));
-    SCC_TRY(get(ctr, sizeof(int32_t) * 2, st));
+    SCC_TRY(get(hub, sizeof(int32_t) * (size_t)n, st));
+    SCC_TRY(get(hubs, sizeof(int32_t) * (size_t)n, st));
+    SCC_TRY(get(hoff, sizeof(long long) * (size_t)n, st));
+    SCC_TRY(get(ctr, sizeof(int32_t) * 4, st));      // overflow count, max level, hub count
     LevelArgs a;
     a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin;
     a.cnt = cnt.as<int32_t>(); a.level = d_level; a.ovf = ovf.as<int32_t>(); a.ovf_count = ctr.as<int32_t>();
+    a.hub = hub.as<int32_t>(); a.hub_count = ctr.as<int32_t>() + 2;
     k_level_init<<<scc_blocks(n), SCC_THREADS, 0, st>>>(n, g->r_begin, a.cnt, d_level);
     SCC_CUDA(cudaPeekAtLastError());
-    SCC_CUDA(cudaMemsetAsync(ctr.p, 0, sizeof(int32_t) * 2, st));
+    SCC_CUDA(cudaMemsetAsync(ctr.p, 0, sizeof(int32_t) * 4, st));
     k_level_peel<<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, st>>>(a, n, nullptr);
     SCC_CUDA(cudaPeekAtLastError());
-    // each node is released once, so the overflow lists together hold at most n
+    // Rounds: overflowed releases expanded by a list launch, hubs edge-parallel
+    // (their releases join the overflow list).  Each node is released once,
+    // so the lists together hold at most n and the rounds end.
     for (int round = 0; round < 1000000; ++round) {
-        int32_t novf = 0;
-        SCC_CUDA(cudaMemcpyAsync(&novf, ctr.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        int32_t c[4] = {0, 0, 0, 0};
+        SCC_CUDA(cudaMemcpyAsync(c, ctr.p, sizeof(c), cudaMemcpyDeviceToHost, st));
         SCC_CUDA(cudaStreamSynchronize(st));
-        if (novf == 0) break;
-        SCC_CUDA(cudaMemcpyAsync(list.p, ovf.p, sizeof(int32_t) * (size_t)novf, cudaMemcpyDeviceToDevice, st));
+        const int32_t novf = c[0], nhub = c[2];
+        if (novf == 0 && nhub == 0) break;
+        if (novf > 0)
+            SCC_CUDA(cudaMemcpyAsync(list.p, ovf.p, sizeof(int32_t) * (size_t)novf, cudaMemcpyDeviceToDevice, st));
+        if (nhub > 0)
+            SCC_CUDA(cudaMemcpyAsync(hubs.p, hub.p, sizeof(int32_t) * (size_t)nhub, cudaMemcpyDeviceToDevice, st));
         SCC_CUDA(cudaMemsetAsync(ctr.p, 0, sizeof(int32_t), st));
-        k_level_peel<<<scc_blocks(novf, SCC_THREADS, 148 * 8), SCC_THREADS, 0, st>>>(a, novf, list.as<int32_t>());
-        SCC_CUDA(cudaPeekAtLastError());
+        SCC_CUDA(cudaMemsetAsync(ctr.as<int32_t>() + 2, 0, sizeof(int32_t), st));
+        if (nhub > 0) {
+            k_level_hub_prefix<<<1, 1024, 0, st>>>(g->begin, hubs.as<int32_t>(), nhub, hoff.as<long long>());
+            SCC_CUDA(cudaPeekAtLastError());
+            k_level_hub<<<148 * 8, SCC_THREADS, 0, st>>>(a, hubs.as<int32_t>(), nhub, hoff.as<long long>());
+            SCC_CUDA(cudaPeekAtLastError());
+        }
+        if (novf > 0) {
+            k_level_peel<<<scc_blocks(novf, SCC_THREADS, 148 * 8), SCC_THREADS, 0, st>>>(a, novf, list.as<int32_t>());
+            SCC_CUDA(cudaPeekAtLastError());
+        }
     }
     int32_t* d_max = ctr.as<int32_t>() + 1;
     k_level_max<<<scc_blocks(n), SCC_THREADS, 0, st>>>(n, d_level, d_max);
@@ -312,6 +391,7 @@ extern "C" int scc_state_finish_unaffected(scc_state* s, const int32_t* levels, 
         SCC_LAUNCHED(s);
     }
     SCC_TRY(scc_sync_counters(s));
+    s->prefinished = s->fresh || s->prefinished;   // the counting peel still applies
     s->fresh = false;
     s->cnt_valid = false;
     if (finished) *finished = s->h_ctr[CTR_COUNT];

@@ -566,8 +566,11 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
     if (live_edges == 0) live_edges = 1;
     // a small round (at most 4x the drain's entry threshold of live vertices)
     // goes straight to the drain: its frontier cannot outgrow the drain, and
-    // level steps would cost a launch and a host round trip each
-    int narrow = ((int64_t)a.live_count <= 4LL * s->tune.async_max) ? s->tune.async_after : 0;
+    // level steps would cost a launch and a host round trip each -- unless it
+    // holds a hub, which a drain warp would expand alone while the level
+    // kernels expand it over the whole grid
+    int narrow = ((int64_t)a.live_count <= 4LL * s->tune.async_max && s->h_ctr[CTR_MAXDEG] <= a.huge_deg)
+                     ? s->tune.async_after : 0;
     bool bottom_up = false;
     double t0 = scc_trace_on() ? now_ms() : 0.0;
     while (qlen > 0) {

@@ -209,6 +209,7 @@ extern "C" int scc_state_reset(scc_state* s) {
     SCC_CUDA(cudaStreamSynchronize(s->stream));
     s->live_count = -1;
     s->fresh = true;
+    s->prefinished = false;
     s->cnt_valid = false;
     s->wq_colors.clear();
     s->wq_counts.clear();
@@ -340,6 +341,7 @@ static int copy_out(scc_state* s, int32_t* host, const int32_t* dev) {
 static int copy_in(scc_state* s, int32_t* dev, const int32_t* host) {
     SCC_REQUIRE(s && host, SCC_ERR_INVALID, "NULL argument");
     s->fresh = false;
+    s->prefinished = false;
     SCC_CUDA(cudaSetDevice(s->device));
     if (s->n > 0) SCC_CUDA(cudaMemcpyAsync(dev, host, sizeof(int32_t) * (size_t)s->n, cudaMemcpyHostToDevice, s->stream));
     SCC_CUDA(cudaStreamSynchronize(s->stream));

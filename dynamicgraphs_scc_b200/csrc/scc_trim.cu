@@ -177,6 +177,8 @@ __global__ void k_trim1_fresh(TrimArgs a, int32_t n) {
 // per edge to a trimmed neighbour, so it never borrows), and the result is
 // the same fixpoint as the scanning peel.
 #define SCC_COLOR_SEED (-3)
+#define SCC_COLOR_PREDONE (-4)    // finished before the peel: expanded by the sweep, not trimmed again
+#define CNT_NEVER 0x7FFFFFFF7FFFFFFFull   // a finished vertex's counts: no decrement brings a half to zero
 
 __device__ __forceinline__ int32_t self_run(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                                             int32_t v) {
@@ -192,11 +194,19 @@ __device__ __forceinline__ int32_t self_run(const int32_t* __restrict__ off, con
 
 // Live-degree counts; the self-loop runs are looked up only when the graph has
 // self-loops (graphs built without them skip the adjacency reads entirely).
+// prefinished: vertices already finished (colour -2) count as trimmed; the
+// sweep expands them, so their live neighbours' counts come out exact.
 __global__ void k_count_init(const int32_t* __restrict__ begin, const int32_t* __restrict__ node_idx,
                              const int32_t* __restrict__ r_begin, const int32_t* __restrict__ r_node_idx, int32_t n,
-                             int has_self, unsigned long long* __restrict__ cnt, int32_t* __restrict__ color) {
+                             int has_self, unsigned long long* __restrict__ cnt, int32_t* __restrict__ color,
+                             int prefinished) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         int32_t v = (int32_t)i;
+        if (prefinished && color[v] == SCC_COLOR_DONE) {
+            cnt[v] = CNT_NEVER;
+            color[v] = SCC_COLOR_PREDONE;
+            continue;
+        }
         int32_t co = __ldg(begin + v + 1) - __ldg(begin + v), ci = __ldg(r_begin + v + 1) - __ldg(r_begin + v);
         if (has_self) {
             co -= self_run(begin, node_idx, v);
@@ -232,10 +242,37 @@ struct CountArgs {
     const int32_t* begin; const int32_t* node_idx; const int32_t* r_begin; const int32_t* r_node_idx;
     int32_t* color; int32_t* scc; unsigned long long* cnt;
     int32_t* ovf; int32_t* ctr;
+    int32_t* hub;           // trimmed vertices above PEEL_HUB edges, expanded edge-parallel (count CTR_SPARE3)
 };
 
 #define PEEL_Q 256          // per-warp queue of trimmed vertices awaiting expansion
+#define PEEL_HUB 4096       // a trimmed vertex with more edges is not expanded by one warp
 #define CNT_IN_ONE (1ull << 32)
+
+// One edge of trimmed x: out-edges take an in-neighbour from w, in-edges an
+// out-neighbour; returns the neighbour this decrement trims, or -1.
+__device__ __forceinline__ int32_t peel_edge(const CountArgs& a, int32_t x, int32_t ob, int32_t od, int32_t ib,
+                                             int32_t k) {
+    int32_t nv = -1;
+    if (k < od) {
+        int32_t w = __ldg(a.node_idx + ob + k);
+        if (w != x) {
+            unsigned long long old = atomicAdd(a.cnt + w, 0ull - CNT_IN_ONE);
+            if ((old >> 32) == 1ull && (uint32_t)old != 0u) nv = w;
+        }
+    } else {
+        int32_t u = __ldg(a.r_node_idx + ib + (k - od));
+        if (u != x) {
+            unsigned long long old = atomicAdd(a.cnt + u, 0ull - 1ull);
+            if ((uint32_t)old == 1u && (old >> 32) != 0ull) nv = u;
+        }
+    }
+    if (nv >= 0) {
+        a.color[nv] = SCC_COLOR_DONE;
+        a.scc[nv] = nv;
+    }
+    return nv;
+}
 
 // Expand this warp's queued trimmed vertices, 32 at a time, with their edges
 // spread over the lanes (a warp prefix sum of the degrees; each lane finds the
@@ -256,6 +293,12 @@ __device__ void peel_drain(const CountArgs& a, int32_t* wq, int32_t& qn, int32_t
         if (x >= 0) {
             ob = __ldg(a.begin + x); od = __ldg(a.begin + x + 1) - ob;
             ib = __ldg(a.r_begin + x); id = __ldg(a.r_begin + x + 1) - ib;
+            if (od + id > PEEL_HUB) {
+                // one warp would take od + id atomics' round trips: the host
+                // expands it over the whole grid instead
+                a.hub[atomicAdd(a.ctr + CTR_SPARE3, 1)] = x;
+                od = id = 0;
+            }
         }
         const int32_t d = od + id;
         int32_t incl = d;
@@ -278,27 +321,7 @@ __device__ void peel_drain(const CountArgs& a, int32_t* wq, int32_t& qn, int32_t
             const int32_t oob = __shfl_sync(full, ob, owner), ood = __shfl_sync(full, od, owner);
             const int32_t oib = __shfl_sync(full, ib, owner);
             int32_t nv = -1;
-            if (j < total) {
-                if (k < ood) {
-                    // out-neighbour w loses an in-neighbour: high half
-                    int32_t w = __ldg(a.node_idx + oob + k);
-                    if (w != ox) {
-                        unsigned long long old = atomicAdd(a.cnt + w, 0ull - CNT_IN_ONE);
-                        if ((old >> 32) == 1ull && (uint32_t)old != 0u) nv = w;
-                    }
-                } else {
-                    // in-neighbour u loses an out-neighbour: low half
-                    int32_t u = __ldg(a.r_node_idx + oib + (k - ood));
-                    if (u != ox) {
-                        unsigned long long old = atomicAdd(a.cnt + u, 0ull - 1ull);
-                        if ((uint32_t)old == 1u && (old >> 32) != 0ull) nv = u;
-                    }
-                }
-                if (nv >= 0) {
-                    a.color[nv] = SCC_COLOR_DONE;
-                    a.scc[nv] = nv;
-                }
-            }
+            if (j < total) nv = peel_edge(a, ox, oob, ood, oib, k);
             const unsigned bal = __ballot_sync(full, nv >= 0);
             if (bal) {
                 const int32_t r = __popc(bal & ((1u << lane) - 1u)), nn = __popc(bal);
@@ -336,11 +359,15 @@ __global__ void __launch_bounds__(SCC_THREADS) k_count_peel(CountArgs a, int32_t
             } else {
                 // only the sweep writes a seed's colour, so a plain read decides
                 int32_t v = (int32_t)i;
-                if (a.color[v] == SCC_COLOR_SEED) {
+                const int32_t c = a.color[v];
+                if (c == SCC_COLOR_SEED) {
                     a.color[v] = SCC_COLOR_DONE;
                     a.scc[v] = v;
                     x = v;
                     cnt++;
+                } else if (c == SCC_COLOR_PREDONE) {     // finished already: expand only
+                    a.color[v] = SCC_COLOR_DONE;
+                    x = v;
                 }
             }
         }
@@ -353,35 +380,115 @@ __global__ void __launch_bounds__(SCC_THREADS) k_count_peel(CountArgs a, int32_t
     block_count_add(a.ctr + CTR_COUNT, cnt);
 }
 
+// Inclusive prefix of the hubs' edge counts (one block; hoff[j] = end of hub j).
+__global__ void k_hub_prefix(const int32_t* __restrict__ begin, const int32_t* __restrict__ r_begin,
+                             const int32_t* __restrict__ hubs, int32_t cnt, long long* __restrict__ hoff) {
+    __shared__ long long part[1024];
+    int t = threadIdx.x;
+    int32_t per = (cnt + 1023) / 1024;
+    int32_t b = t * per, e = min(cnt, b + per);
+    long long sum = 0;
+    for (int32_t j = b; j < e; ++j) {
+        int32_t x = hubs[j];
+        sum += (long long)(__ldg(begin + x + 1) - __ldg(begin + x)) + (__ldg(r_begin + x + 1) - __ldg(r_begin + x));
+    }
+    part[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        long long v = (t >= o) ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    long long run = (t == 0) ? 0 : part[t - 1];
+    for (int32_t j = b; j < e; ++j) {
+        int32_t x = hubs[j];
+        run += (long long)(__ldg(begin + x + 1) - __ldg(begin + x)) + (__ldg(r_begin + x + 1) - __ldg(r_begin + x));
+        hoff[j] = run;
+    }
+}
+
+// Edge-parallel expansion of trimmed hubs: thread t takes edge t of their
+// concatenated lists; trims it causes go to the overflow list, expanded by the
+// next list launch of k_count_peel.
+__global__ void k_hub_peel(CountArgs a, const int32_t* __restrict__ hubs, int32_t cnt,
+                           const long long* __restrict__ hoff) {
+    const long long total = hoff[cnt - 1];
+    int32_t trims = 0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long limit = ((total + 31) / 32) * 32;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < limit; t += stride) {
+        int32_t nv = -1;
+        if (t < total) {
+            int32_t lo = 0, hi = cnt - 1;
+            while (lo < hi) { int32_t mid = (lo + hi) >> 1; if (hoff[mid] > t) hi = mid; else lo = mid + 1; }
+            const int32_t x = hubs[lo];
+            const long long start = lo ? hoff[lo - 1] : 0;
+            const int32_t ob = __ldg(a.begin + x), od = __ldg(a.begin + x + 1) - ob, ib = __ldg(a.r_begin + x);
+            nv = peel_edge(a, x, ob, od, ib, (int32_t)(t - start));
+        }
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, nv >= 0);
+        if (bal) {
+            const int lane = threadIdx.x & 31;
+            int32_t base = 0;
+            if (lane == 0) base = atomicAdd(a.ctr + CTR_OVERFLOW, __popc(bal));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (nv >= 0) a.ovf[base + __popc(bal & ((1u << lane) - 1u))] = nv;
+            trims += nv >= 0;
+        }
+    }
+    block_count_add(a.ctr + CTR_COUNT, trims);
+}
+
 static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     int32_t n = g->n;
     CountArgs a;
     a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin; a.r_node_idx = g->r_node_idx;
     a.color = s->color; a.scc = s->scc; a.cnt = s->cnt;
-    a.ovf = s->qa; a.ctr = s->ctr;
+    a.ovf = s->qa; a.ctr = s->ctr; a.hub = s->hq;
     SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
     SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
+    SCC_TRY(scc_zero_counters(s, CTR_SPARE3, 1));
     SCC_TRY(count_self_loops(g, s));
     k_count_init<<<scc_blocks(n), SCC_THREADS, 0, s->stream>>>(g->begin, g->node_idx, g->r_begin, g->r_node_idx, n,
-                                                               g->self_loops > 0 ? 1 : 0, s->cnt, s->color);
+                                                               g->self_loops > 0 ? 1 : 0, s->cnt, s->color,
+                                                               s->prefinished ? 1 : 0);
     SCC_LAUNCHED(s);
     k_count_peel<<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, n, nullptr);
     SCC_LAUNCHED(s);
     int64_t total = 0;
+    // Rounds: overflowed trims are expanded by a list launch, hubs edge-parallel
+    // (their trims join the overflow list).  Every vertex is trimmed once, so
+    // the lists together never exceed n and the rounds end.
     for (int round = 0; round < 1000000; ++round) {
         SCC_TRY(scc_sync_counters(s));
         total += s->h_ctr[CTR_COUNT];
         int32_t novf = s->h_ctr[CTR_OVERFLOW];
-        if (novf == 0) break;
-        SCC_CUDA(cudaMemcpyAsync(s->qb, s->qa, sizeof(int32_t) * (size_t)novf, cudaMemcpyDeviceToDevice, s->stream));
+        int32_t nhub = s->h_ctr[CTR_SPARE3];
+        if (novf == 0 && nhub == 0) break;
         SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
+        if (novf > 0)
+            SCC_CUDA(cudaMemcpyAsync(s->qb, s->qa, sizeof(int32_t) * (size_t)novf, cudaMemcpyDeviceToDevice, s->stream));
+        if (nhub > 0)
+            SCC_CUDA(cudaMemcpyAsync(s->aux, s->hq, sizeof(int32_t) * (size_t)nhub, cudaMemcpyDeviceToDevice, s->stream));
         SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
-        k_count_peel<<<scc_blocks(novf, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, novf, s->qb);
-        SCC_LAUNCHED(s);
+        SCC_TRY(scc_zero_counters(s, CTR_SPARE3, 1));
+        if (nhub > 0) {
+            k_hub_prefix<<<1, 1024, 0, s->stream>>>(g->begin, g->r_begin, s->aux, nhub, s->hoff);
+            SCC_LAUNCHED(s);
+            k_hub_peel<<<148 * 8, SCC_THREADS, 0, s->stream>>>(a, s->aux, nhub, s->hoff);
+            SCC_LAUNCHED(s);
+        }
+        if (novf > 0) {
+            k_count_peel<<<scc_blocks(novf, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, novf, s->qb);
+            SCC_LAUNCHED(s);
+        }
     }
     *trimmed = (int32_t)total;
+    s->cnt_valid = !s->prefinished;      // the residue of finished vertices is not a count
     s->fresh = false;
-    s->cnt_valid = true;
+    s->prefinished = false;
+    s->prefinished = false;
     return SCC_OK;
 }
 
@@ -404,6 +511,57 @@ __global__ void k_trim1_overflow(TrimArgs a, const int32_t* __restrict__ items, 
                 int32_t w = __ldg(adj + k);
                 if (w != x && try_trim(a, g, w, c)) { cnt++; cascade(a, g, w, c, cnt); }
             }
+        }
+    }
+    block_count_add(a.ctr + CTR_COUNT, cnt);
+}
+
+// Edge-parallel overflow expansion (the engine's own peel): thread t takes edge
+// t of the overflowed vertices' concatenated out- and in-lists, so a hub's
+// neighbours are re-checked by the whole grid instead of one warp.
+__global__ void k_ovf_prefix(const int32_t* __restrict__ begin, const int32_t* __restrict__ r_begin,
+                             const int32_t* __restrict__ items, int32_t cnt, long long* __restrict__ hoff) {
+    __shared__ long long part[1024];
+    int t = threadIdx.x;
+    int32_t per = (cnt + 1023) / 1024;
+    int32_t b = t * per, e = min(cnt, b + per);
+    long long sum = 0;
+    for (int32_t j = b; j < e; ++j) {
+        int32_t x = items[j];
+        sum += (long long)(__ldg(begin + x + 1) - __ldg(begin + x)) + (__ldg(r_begin + x + 1) - __ldg(r_begin + x));
+    }
+    part[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        long long v = (t >= o) ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    long long run = (t == 0) ? 0 : part[t - 1];
+    for (int32_t j = b; j < e; ++j) {
+        int32_t x = items[j];
+        run += (long long)(__ldg(begin + x + 1) - __ldg(begin + x)) + (__ldg(r_begin + x + 1) - __ldg(r_begin + x));
+        hoff[j] = run;
+    }
+}
+
+__global__ void k_trim1_overflow_edges(TrimArgs a, const int32_t* __restrict__ items, int32_t n_items,
+                                       const int32_t* __restrict__ item_colors, const long long* __restrict__ hoff) {
+    scc_graph g = as_graph(a);
+    int32_t cnt = 0;
+    const long long total = hoff[n_items - 1];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long limit = ((total + 31) / 32) * 32;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < limit; t += stride) {
+        if (t < total) {
+            int32_t lo = 0, hi = n_items - 1;
+            while (lo < hi) { int32_t mid = (lo + hi) >> 1; if (hoff[mid] > t) hi = mid; else lo = mid + 1; }
+            const int32_t x = items[lo], c = item_colors[lo];
+            const int32_t k = (int32_t)(t - (lo ? hoff[lo - 1] : 0));
+            const int32_t ob = __ldg(a.begin + x), od = __ldg(a.begin + x + 1) - ob;
+            const int32_t w = k < od ? __ldg(a.node_idx + ob + k) : __ldg(a.r_node_idx + __ldg(a.r_begin + x) + (k - od));
+            if (w != x && try_trim(a, g, w, c)) { cnt++; cascade(a, g, w, c, cnt); }
         }
     }
     block_count_add(a.ctr + CTR_COUNT, cnt);
@@ -443,8 +601,9 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
     *trimmed = 0;
     if (n_items <= 0) return SCC_OK;
     // snapshot colours (aux) so overflowed vertices keep their pre-trim colour
+    if ((s->fresh || s->prefinished) && !use_live && s->cnt) return trim1_counting(g, s, trimmed);
+    s->prefinished = false;
     bool fresh = s->fresh && !use_live;
-    if (fresh && s->cnt) return trim1_counting(g, s, trimmed);
     if (fresh) {
         // every colour is -1: the snapshot the overflow path reads is that constant
         k_fill_aux<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(n_items, s->aux, SCC_COLOR_INIT);
@@ -466,6 +625,7 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
         k_trim1_sweep<<<scc_blocks(n_items, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, list, n_items);
     SCC_LAUNCHED(s);
     s->fresh = false;
+    s->prefinished = false;
     int64_t total = 0;
     for (int round = 0; round < 1000000; ++round) {
         SCC_TRY(scc_sync_counters(s));
@@ -478,8 +638,9 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
         SCC_LAUNCHED(s);
         SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
         SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
-        k_trim1_overflow<<<scc_blocks((int64_t)novf * 32, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(
-            a, s->qb, novf, s->live_tmp);
+        k_ovf_prefix<<<1, 1024, 0, s->stream>>>(g->begin, g->r_begin, s->qb, novf, s->hoff);
+        SCC_LAUNCHED(s);
+        k_trim1_overflow_edges<<<148 * 8, SCC_THREADS, 0, s->stream>>>(a, s->qb, novf, s->live_tmp, s->hoff);
         SCC_LAUNCHED(s);
     }
     *trimmed = (int32_t)total;
@@ -586,6 +747,7 @@ __global__ void k_trim2_apply(int32_t* __restrict__ color, int32_t* __restrict__
 int scc_impl_trim2(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     *trimmed = 0;
     s->fresh = false;
+    s->prefinished = false;
     bool use_live = s->live_count >= 0;
     int64_t n_items = use_live ? s->live_count : g->n;
     const int32_t* list = use_live ? s->live : nullptr;

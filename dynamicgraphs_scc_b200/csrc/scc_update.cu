@@ -373,6 +373,7 @@ extern "C" int scc_update_batch(scc_graph* g, scc_state* s, int64_t n_ins, const
         out.affected_delete = s->h_ctr[CTR_SPARE0];
         if (out.affected_delete > 0) {
             s->fresh = false;
+            s->prefinished = false;
             s->live_count = -1;
             SCC_TRY(scc_impl_resolve_all(g, s));
         }
@@ -396,6 +397,7 @@ extern "C" int scc_update_batch(scc_graph* g, scc_state* s, int64_t n_ins, const
             SCC_TRY(scc_impl_compact_live(g, s, true));
             RoundArgs a = update_round_args(g, s);
             *reinterpret_cast<unsigned long long*>(s->h_ctr + CTR_LIVE_EDGES) = 2ull * (unsigned long long)g->m;
+            s->h_ctr[CTR_MAXDEG] = INT32_MAX;      // degrees not scanned here: no shortcut to the drain
             SCC_TRY(scc_impl_reach(g, s, a, qlen));
             SCC_TRY(scc_zero_counters(s, CTR_SPARE0, 1));
             k_upd_colour_region<<<scc_blocks(n), SCC_THREADS, 0, st>>>(n, s->mark, s->color, s->ctr + CTR_SPARE0);
@@ -403,6 +405,7 @@ extern "C" int scc_update_batch(scc_graph* g, scc_state* s, int64_t n_ins, const
             SCC_TRY(scc_sync_counters(s));
             out.affected_insert = s->h_ctr[CTR_SPARE0];
             s->fresh = false;
+            s->prefinished = false;
             s->live_count = -1;
             if (out.affected_insert > 0) SCC_TRY(scc_impl_resolve_all(g, s));
         } else {

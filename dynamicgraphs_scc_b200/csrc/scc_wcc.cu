@@ -136,6 +136,7 @@ __global__ void k_member_color(const int32_t* __restrict__ live, int32_t n_items
 
 int scc_impl_wcc(const scc_graph* g, scc_state* s) {
     s->fresh = false;
+    s->prefinished = false;
     if (s->live_count < 0) SCC_TRY(scc_impl_compact_live(g, s, true));
     int32_t n_items = s->live_count;
     if (n_items <= 0) return SCC_OK;
@@ -264,6 +265,7 @@ __global__ void k_uf_flatten(const int32_t* __restrict__ live, int32_t n_items, 
 // overwritten, so colour ids stay below n.
 int scc_impl_uf_split(const scc_graph* g, scc_state* s, int32_t* num_classes) {
     s->fresh = false;
+    s->prefinished = false;
     int32_t n_items = s->live_count;
     *num_classes = 0;
     if (n_items <= 0) return SCC_OK;

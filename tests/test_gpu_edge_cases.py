@@ -89,3 +89,57 @@ def test_very_long_cycle_completes(gpu):
     assert r["num_sccs"] == 1 and r["first_scc_size"] == n
     assert not st.canonical_labels().any()
     st.free(); g.free()
+
+
+def _hub_graph():
+    rng = np.random.default_rng(51)
+    leaves = 200000
+    base = 10000
+    s_r, d_r = rng.integers(0, base, 30000), rng.integers(0, base, 30000)
+    h1 = base
+    l1 = np.arange(base + 1, base + 1 + leaves)
+    src = base + 1 + leaves
+    h2 = src + 1
+    l2 = np.arange(h2 + 1, h2 + 1 + leaves)
+    h3 = h2 + 1 + leaves
+    n = h3 + 1
+    s = np.concatenate([s_r, np.full(leaves, h1), [src], np.full(leaves, h2), l2, rng.integers(0, base, 50)])
+    d = np.concatenate([d_r, l1, [h2], l2, np.full(leaves, h3), np.full(50, h1)])
+    return n, s, d
+
+
+def test_scanning_peel_hubs_edge_parallel(gpu):
+    # the same hubs through the peel of a state that is not fresh (colours
+    # given explicitly), whose overflowed vertices are re-checked over the grid
+    n, s, d = _hub_graph()
+    csr = O.build_csr(n, np.asarray(s, np.int32), np.asarray(d, np.int32))
+    exp = O.tarjan_canonical(csr[0], csr[1])
+    g = Graph.from_edges(n, np.asarray(s, np.int32), np.asarray(d, np.int32))
+    st = State(g)
+    for method in (0, 2):
+        st.reset()
+        st.set_color(np.full(n, -1, np.int32))
+        st.run(method)
+        assert np.array_equal(st.canonical_labels(), exp), method
+    st.free(); g.free()
+
+
+def test_peel_hubs_expanded_edge_parallel(gpu):
+    # a source hub with 200,000 out-edges (trimmed as a seed), a hub reached
+    # from a source by one edge (trimmed by a cascade), a sink hub with
+    # 200,000 in-edges, and a random graph with real SCCs beside them: hubs
+    # above 4,096 edges are expanded over the whole grid, not by one warp
+    rng = np.random.default_rng(51)
+    leaves = 200000
+    base = 10000
+    s_r, d_r = rng.integers(0, base, 30000), rng.integers(0, base, 30000)
+    h1 = base
+    l1 = np.arange(base + 1, base + 1 + leaves)
+    src = base + 1 + leaves
+    h2 = src + 1
+    l2 = np.arange(h2 + 1, h2 + 1 + leaves)
+    h3 = h2 + 1 + leaves
+    n = h3 + 1
+    s = np.concatenate([s_r, np.full(leaves, h1), [src], np.full(leaves, h2), l2, rng.integers(0, base, 50)])
+    d = np.concatenate([d_r, l1, [h2], l2, np.full(leaves, h3), np.full(50, h1)])
+    _check(n, s, d)

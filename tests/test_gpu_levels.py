@@ -104,3 +104,48 @@ def test_affected_levels_rejects_bad_input(gpu):
     with pytest.raises(SccError):
         affected_levels(g, lev, ml, np.array([0, 1, 9], np.int32), [0], [2])     # label outside [0, 3)
     g.free()
+
+
+def test_levels_hub_released_by_a_chain(gpu):
+    # 0 -> 1 -> 2 (a hub with 50,000 children) -> each child -> a sink: the hub
+    # is released by a cascade, then expanded over the whole grid
+    k = 50000
+    kids = np.arange(3, 3 + k, dtype=np.int32)
+    sink = 3 + k
+    s = np.concatenate([[0, 1], np.full(k, 2), kids]).astype(np.int32)
+    d = np.concatenate([[1, 2], kids, np.full(k, sink)]).astype(np.int32)
+    n = sink + 1
+    g = Graph.from_edges(n, s, d)
+    lev, ml = topological_levels(g)
+    b, a = O.condensation_csr(np.arange(n, dtype=np.int32), n, s, d)
+    exp, exp_max = O.topo_levels(b, a)
+    assert ml == exp_max == 4 and np.array_equal(lev, exp)
+    g.free()
+
+
+def test_method7_flow_with_hubs(gpu):
+    # hubs of 200,000 edges in the condensation: the shortcut's pre-finished
+    # nodes go through the counting peel, hub items leave the asynchronous
+    # drain for the level kernels, and the labels stay exact
+    from tests.test_gpu_edge_cases import _hub_graph
+    n, s, d = _hub_graph()
+    s = np.asarray(s, np.int32); d = np.asarray(d, np.int32)
+    rng = np.random.default_rng(61)
+    ids, k = O.scc_ids(O.tarjan_canonical(*O.build_csr(n, s, d)[:2]))
+    hubs = np.array([10000, 210002, 410003], np.int32)          # the three hubs of the graph
+    isrc = np.concatenate([rng.integers(0, n, 20), hubs[[0, 2]]]).astype(np.int32)
+    idst = np.concatenate([rng.integers(0, n, 20), [hubs[1], hubs[0]]]).astype(np.int32)
+    g = Graph.from_edges(n, s, d)
+    dag = condensation_graph(g, ids, k)
+    lev, ml = topological_levels(dag)
+    aff, z = affected_levels(dag, lev, ml, ids, isrc, idst)
+    cond = condensation_graph(g, ids, k, isrc, idst)
+    st = State(cond)
+    upd = O.tarjan_canonical(*O.build_csr(n, np.concatenate([s, isrc]), np.concatenate([d, idst]))[:2])
+    for shortcut in (True, False):
+        st.reset()
+        if shortcut:
+            st.finish_unaffected(lev, aff, ml)
+        st.run(2)
+        assert np.array_equal(O.canonical(st.canonical_labels()[ids]), upd), shortcut
+    st.free(); cond.free(); dag.free(); g.free()
