@@ -147,15 +147,28 @@ static int bits_for(int32_t n) {
     return b;
 }
 
+// Stream-ordered scratch, released on the same stream.
+struct AsyncScratch {
+    void* p = nullptr;
+    cudaStream_t st;
+    explicit AsyncScratch(cudaStream_t s) : st(s) {}
+    ~AsyncScratch() { if (p) cudaFreeAsync(p, st); }
+    cudaError_t alloc(size_t bytes) { return scc_impl_malloc_async(&p, bytes > 0 ? bytes : 16, st); }
+};
+
 // Sort (hi<<32|lo) keys and write offsets + low words.  keys buffer is reused.
 static int build_side(int32_t n, int64_t m, const int32_t* hi, const int32_t* lo, int flags, cudaStream_t st,
                       int32_t** begin_out, int32_t** idx_out, int64_t* m_out) {
-    unsigned long long *keys = nullptr, *keys2 = nullptr, *dropped = nullptr;
+    // temporaries come from the library's pool, stream-ordered on st (no
+    // device-wide cudaMalloc/cudaFree of GB-sized key buffers per build)
     int64_t mm = m > 0 ? m : 1;
-    SCC_CUDA(cudaMalloc(&keys, sizeof(unsigned long long) * mm));
-    cudaError_t e1 = cudaMalloc(&keys2, sizeof(unsigned long long) * mm);
-    if (e1 != cudaSuccess) { cudaFree(keys); return scc_cuda_status(e1, "cudaMalloc keys2", __FILE__, __LINE__); }
-    SCC_CUDA(cudaMalloc(&dropped, sizeof(unsigned long long) * 2));
+    AsyncScratch keys_b(st), keys2_b(st), dropped_b(st), tmp_b(st), tmp2_b(st), num_b(st);
+    SCC_CUDA(keys_b.alloc(sizeof(unsigned long long) * mm));
+    SCC_CUDA(keys2_b.alloc(sizeof(unsigned long long) * mm));
+    SCC_CUDA(dropped_b.alloc(sizeof(unsigned long long) * 2));
+    unsigned long long* keys = (unsigned long long*)keys_b.p;
+    unsigned long long* keys2 = (unsigned long long*)keys2_b.p;
+    unsigned long long* dropped = (unsigned long long*)dropped_b.p;
     SCC_CUDA(cudaMemsetAsync(dropped, 0, sizeof(unsigned long long) * 2, st));
     int drop_self = (flags & SCC_BUILD_NO_SELF_LOOPS) ? 1 : 0;
     if (m > 0) {
@@ -165,12 +178,10 @@ static int build_side(int32_t n, int64_t m, const int32_t* hi, const int32_t* lo
     int end_bit = 32 + bits_for(n + 1);
     if (drop_self) end_bit = 64;
     size_t tmp_bytes = 0;
-    void* tmp = nullptr;
     cub::DoubleBuffer<unsigned long long> db(keys, keys2);
-    SCC_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, (int)m, 0, end_bit, st));
-    SCC_CUDA(cudaMalloc(&tmp, tmp_bytes > 0 ? tmp_bytes : 16));
-    if (m > 0) SCC_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, (int)m, 0, end_bit, st));
-    cudaFree(tmp);
+    SCC_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, (int)m, 0, end_bit, st));
+    SCC_CUDA(tmp_b.alloc(tmp_bytes));
+    if (m > 0) SCC_CUDA(cub::DeviceRadixSort::SortKeys(tmp_b.p, tmp_bytes, db, (int)m, 0, end_bit, st));
     unsigned long long* sorted = db.Current();
     unsigned long long* other = db.Alternate();
     unsigned long long h_dropped = 0;
@@ -178,30 +189,29 @@ static int build_side(int32_t n, int64_t m, const int32_t* hi, const int32_t* lo
     SCC_CUDA(cudaStreamSynchronize(st));
     int64_t mk = m - (int64_t)h_dropped;   // self-loops sorted to the end
     if ((flags & SCC_BUILD_DEDUP) && mk > 0) {
-        int* d_num = nullptr;
-        SCC_CUDA(cudaMalloc(&d_num, sizeof(int)));
+        SCC_CUDA(num_b.alloc(sizeof(int)));
+        int* d_num = (int*)num_b.p;
         tmp_bytes = 0;
         SCC_CUDA(cub::DeviceSelect::Unique(nullptr, tmp_bytes, sorted, other, d_num, (int)mk, st));
-        SCC_CUDA(cudaMalloc(&tmp, tmp_bytes > 0 ? tmp_bytes : 16));
-        SCC_CUDA(cub::DeviceSelect::Unique(tmp, tmp_bytes, sorted, other, d_num, (int)mk, st));
+        SCC_CUDA(tmp2_b.alloc(tmp_bytes));
+        SCC_CUDA(cub::DeviceSelect::Unique(tmp2_b.p, tmp_bytes, sorted, other, d_num, (int)mk, st));
         int h_num = 0;
         SCC_CUDA(cudaMemcpyAsync(&h_num, d_num, sizeof(int), cudaMemcpyDeviceToHost, st));
         SCC_CUDA(cudaStreamSynchronize(st));
-        cudaFree(tmp); cudaFree(d_num);
         mk = h_num;
         unsigned long long* t = sorted; sorted = other; other = t;
     }
     int32_t *begin = nullptr, *idx = nullptr;
     SCC_CUDA(cudaMalloc(&begin, sizeof(int32_t) * ((size_t)n + 1)));
-    SCC_CUDA(cudaMalloc(&idx, sizeof(int32_t) * (size_t)(mk > 0 ? mk : 1)));
-    SCC_CUDA(fill_offsets(mk, n, sorted, begin, st));
-    SCC_CUDA(cudaPeekAtLastError());
-    if (mk > 0) {
+    cudaError_t e = cudaMalloc(&idx, sizeof(int32_t) * (size_t)(mk > 0 ? mk : 1));
+    if (e != cudaSuccess) { cudaFree(begin); return scc_cuda_status(e, "cudaMalloc", __FILE__, __LINE__); }
+    e = fill_offsets(mk, n, sorted, begin, st);
+    if (e == cudaSuccess && mk > 0) {
         k_low_words<<<scc_blocks(mk, 256, 148 * 64), 256, 0, st>>>(mk, sorted, idx);
-        SCC_CUDA(cudaPeekAtLastError());
+        e = cudaPeekAtLastError();
     }
-    SCC_CUDA(cudaStreamSynchronize(st));
-    cudaFree(keys); cudaFree(keys2); cudaFree(dropped);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { cudaFree(begin); cudaFree(idx); return scc_cuda_status(e, "build_side", __FILE__, __LINE__); }
     *begin_out = begin; *idx_out = idx; *m_out = mk;
     return SCC_OK;
 }
@@ -240,14 +250,6 @@ int scc_impl_build_graph_from_device_edges(int32_t n, int64_t m, const int32_t* 
     return SCC_OK;
 }
 
-// Stream-ordered scratch, released on the same stream.
-struct AsyncScratch {
-    void* p = nullptr;
-    cudaStream_t st;
-    explicit AsyncScratch(cudaStream_t s) : st(s) {}
-    ~AsyncScratch() { if (p) cudaFreeAsync(p, st); }
-    cudaError_t alloc(size_t bytes) { return scc_impl_malloc_async(&p, bytes > 0 ? bytes : 16, st); }
-};
 
 // Transpose of g's forward CSR into g->r_begin / g->r_node_idx (allocated):
 // a stable radix sort of (destination, source) pairs taken in edge order, so
