@@ -22,6 +22,7 @@
 //     R only.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
 #include <algorithm>
 #include <string.h>
 #include "scc_round.cuh"
@@ -504,6 +505,13 @@ __global__ void k_cond_map_batch(int64_t k, const int32_t* __restrict__ a, const
     }
 }
 
+// 1 where an edge joins two different SCCs (the only edges the condensation keeps)
+__global__ void k_cond_flags(int64_t m, const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+                             uint8_t* __restrict__ flags) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+        flags[i] = src[i] != dst[i];
+}
+
 extern "C" int scc_condensation_graph(const scc_graph* g, const int32_t* labels, int32_t num_sccs, int64_t n_ins,
                                       const int32_t* ins_src, const int32_t* ins_dst, scc_graph** out) {
     SCC_REQUIRE(g && labels && out && num_sccs >= 0, SCC_ERR_INVALID, "NULL argument");
@@ -539,8 +547,39 @@ extern "C" int scc_condensation_graph(const scc_graph* g, const int32_t* labels,
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = scc_cuda_status(e, "condensation map", __FILE__, __LINE__);
         else if (hbad) { scc_set_error("label or inserted endpoint out of range"); rc = SCC_ERR_INVALID; }
-        else rc = scc_impl_build_graph_from_device_edges(num_sccs, total, src.as<int32_t>(), dst.as<int32_t>(),
-                                                          SCC_BUILD_DEDUP | SCC_BUILD_NO_SELF_LOOPS, g->device, out);
+        else {
+            // intra-SCC pairs would become self-loops the build drops: compact
+            // the cross-SCC pairs first, so the build sorts only those
+            DevBuf flags, src2, dst2, num, tmp;
+            size_t tb = 0;
+            if ((rc = alloc(flags, (size_t)total, st)) == SCC_OK &&
+                (rc = alloc(src2, sizeof(int32_t) * (size_t)total, st)) == SCC_OK &&
+                (rc = alloc(dst2, sizeof(int32_t) * (size_t)total, st)) == SCC_OK &&
+                (rc = alloc(num, sizeof(int32_t), st)) == SCC_OK) {
+                int32_t hnum = 0;
+                k_cond_flags<<<scc_blocks(total, SCC_THREADS, 148 * 16), SCC_THREADS, 0, st>>>(
+                    total, src.as<int32_t>(), dst.as<int32_t>(), flags.as<uint8_t>());
+                e = cudaPeekAtLastError();
+                if (e == cudaSuccess)
+                    e = cub::DeviceSelect::Flagged(nullptr, tb, src.as<int32_t>(), flags.as<uint8_t>(), src2.as<int32_t>(),
+                                                   num.as<int32_t>(), (int)total, st);
+                if (e == cudaSuccess && (rc = alloc(tmp, tb, st)) == SCC_OK) {
+                    e = cub::DeviceSelect::Flagged(tmp.p, tb, src.as<int32_t>(), flags.as<uint8_t>(), src2.as<int32_t>(),
+                                                   num.as<int32_t>(), (int)total, st);
+                    if (e == cudaSuccess)
+                        e = cub::DeviceSelect::Flagged(tmp.p, tb, dst.as<int32_t>(), flags.as<uint8_t>(),
+                                                       dst2.as<int32_t>(), num.as<int32_t>(), (int)total, st);
+                    if (e == cudaSuccess) e = cudaMemcpyAsync(&hnum, num.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+                    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                    if (e != cudaSuccess) rc = scc_cuda_status(e, "condensation compaction", __FILE__, __LINE__);
+                    else rc = scc_impl_build_graph_from_device_edges(num_sccs, hnum, src2.as<int32_t>(), dst2.as<int32_t>(),
+                                                                      SCC_BUILD_DEDUP | SCC_BUILD_NO_SELF_LOOPS,
+                                                                      g->device, out);
+                } else if (e != cudaSuccess) {
+                    rc = scc_cuda_status(e, "condensation compaction", __FILE__, __LINE__);
+                }
+            }
+        }
     }
     }
     cudaStreamSynchronize(st);
