@@ -20,9 +20,9 @@
 //     every merged SCC lies in R = FW(those v) and BW(those u).  R is a union
 //     of classes closed under strong connectivity; SCCs are recomputed inside
 //     R only.
+#include <cub/block/block_scan.cuh>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
-#include <cub/device/device_select.cuh>
 #include <algorithm>
 #include <string.h>
 #include "scc_round.cuh"
@@ -478,108 +478,189 @@ extern "C" int scc_insert_idea1(scc_graph* g, scc_state* s, int64_t n_ins, const
 // src/scc_incremental.cc:19-27): the condensation graph over the SCC ids of
 // `labels` (ids < num_sccs), with every cross-SCC edge of g and of the
 // inserted batch mapped to (id(u), id(v)); duplicates dropped.
-__global__ void k_cond_map(int32_t n, const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
-                           const int32_t* __restrict__ label, int32_t num_sccs, int32_t* __restrict__ src,
-                           int32_t* __restrict__ dst, int* __restrict__ bad) {
-    int lane = threadIdx.x & 31;
-    int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < n; w += wstride) {
-        int32_t v = (int32_t)w;
-        int32_t lv = label[v];
-        if (lane == 0 && (lv < 0 || lv >= num_sccs)) atomicExch(bad, 1);
-        for (int32_t k = off[v] + lane; k < off[v + 1]; k += 32) {
-            src[k] = lv;                 // intra-SCC pairs become self-loops, dropped by the build
-            dst[k] = label[adj[k]];
-        }
+// Condensation edges (create_scc_edges, src/common_main.h:180-314): every
+// edge (u, v) becomes (label[u], label[v]); pairs inside one SCC would be
+// self-loops the build drops, so only cross-SCC pairs are written, appended
+// to a compact list.  Edge-balanced: a block takes COND_CHUNK consecutive
+// edges, stages the offsets and labels of the vertices owning them in shared
+// memory, and each thread finds its edges' sources there by binary search.
+// Adjacency is streamed (evict-first) so the label array stays in L2 for
+// the random destination gathers.
+#define COND_ITEMS 8
+#define COND_CHUNK (SCC_THREADS * COND_ITEMS)
+#define COND_TILE_V COND_CHUNK
+
+// largest v in [lo, hi] with off[v] <= k (off[lo] <= k)
+__device__ __forceinline__ int32_t cond_owner(const int32_t* off, int32_t lo, int32_t hi, int32_t k) {
+    while (lo < hi) {
+        int32_t mid = lo + ((hi - lo + 1) >> 1);
+        if (off[mid] <= k) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// owner[c] = source vertex of edge c * COND_CHUNK; owner[chunks] = n - 1
+__global__ void k_cond_owners(int32_t n, int64_t chunks, const int32_t* __restrict__ off, int32_t* __restrict__ owner) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c <= chunks; c += (int64_t)gridDim.x * blockDim.x)
+        owner[c] = c == chunks ? n - 1 : cond_owner(off, 0, n - 1, (int32_t)(c * COND_CHUNK));
+}
+
+__global__ void k_cond_check_labels(int32_t n, const int32_t* __restrict__ label, int32_t num_sccs, int* __restrict__ bad) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        int32_t l = label[v];
+        if (l < 0 || l >= num_sccs) atomicExch(bad, 1);
     }
 }
 
-__global__ void k_cond_map_batch(int64_t k, const int32_t* __restrict__ a, const int32_t* __restrict__ b,
-                                 const int32_t* __restrict__ label, int32_t n, int32_t* __restrict__ src,
-                                 int32_t* __restrict__ dst, int* __restrict__ bad) {
+__global__ void __launch_bounds__(SCC_THREADS) k_cond_cross(int32_t m, int64_t chunks, const int32_t* __restrict__ off,
+                                                            const int32_t* __restrict__ adj,
+                                                            const int32_t* __restrict__ label,
+                                                            const int32_t* __restrict__ owner,
+                                                            int32_t* __restrict__ out_src, int32_t* __restrict__ out_dst,
+                                                            int32_t* __restrict__ count) {
+    using Scan = cub::BlockScan<int, SCC_THREADS>;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    __shared__ int32_t s_off[COND_TILE_V + 1];
+    __shared__ int32_t s_lab[COND_TILE_V];
+    __shared__ int32_t s_base;
+    const bool vec = (((uintptr_t)adj) & 15) == 0;
+    for (int64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+        const int32_t e0 = (int32_t)(c * COND_CHUNK);
+        const int32_t e1 = (int32_t)min((int64_t)m, (c + 1) * COND_CHUNK);
+        const int32_t vs = owner[c], hi = owner[c + 1];   // every source of the chunk lies in [vs, hi]
+        const int32_t nv = hi - vs + 1;
+        const bool tiled = nv <= COND_TILE_V;
+        if (tiled) {
+            for (int i = threadIdx.x; i <= nv; i += SCC_THREADS) s_off[i] = off[vs + i];
+            for (int i = threadIdx.x; i < nv; i += SCC_THREADS) s_lab[i] = label[vs + i];
+        }
+        const int32_t k0 = e0 + threadIdx.x * COND_ITEMS;
+        int32_t d[COND_ITEMS];
+        if (vec && k0 + COND_ITEMS <= e1) {
+#pragma unroll
+            for (int j = 0; j < COND_ITEMS; j += 4) {
+                int4 q = __ldcs((const int4*)(adj + k0 + j));
+                d[j] = q.x; d[j + 1] = q.y; d[j + 2] = q.z; d[j + 3] = q.w;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < COND_ITEMS; j++) d[j] = k0 + j < e1 ? __ldcs(adj + k0 + j) : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < COND_ITEMS; j++) d[j] = k0 + j < e1 ? __ldg(label + d[j]) : 0;
+        __syncthreads();
+        int32_t sl[COND_ITEMS];
+        int keep = 0;
+        if (k0 < e1) {
+            if (tiled) {
+                int32_t i = cond_owner(s_off, 0, nv - 1, k0);
+#pragma unroll
+                for (int j = 0; j < COND_ITEMS; j++) {
+                    sl[j] = 0;
+                    if (k0 + j < e1) {   // off[hi + 1] > k0 + j stops the walk inside the tile
+                        while (s_off[i + 1] <= k0 + j) i++;
+                        sl[j] = s_lab[i];
+                    }
+                }
+            } else {
+                int32_t v = cond_owner(off, vs, hi, k0);
+#pragma unroll
+                for (int j = 0; j < COND_ITEMS; j++) {
+                    sl[j] = 0;
+                    if (k0 + j < e1) {
+                        while (v < hi && off[v + 1] <= k0 + j) v++;
+                        sl[j] = label[v];
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < COND_ITEMS; j++)
+                if (k0 + j < e1 && sl[j] != d[j]) keep |= 1 << j;
+        }
+        int pre, total;
+        Scan(scan_tmp).ExclusiveSum(__popc(keep), pre, total);
+        if (threadIdx.x == 0 && total > 0) s_base = atomicAdd(count, total);
+        __syncthreads();
+        if (keep) {
+            int32_t at = s_base + pre;
+#pragma unroll
+            for (int j = 0; j < COND_ITEMS; j++)
+                if (keep & (1 << j)) { out_src[at] = sl[j]; out_dst[at] = d[j]; at++; }
+        }
+        __syncthreads();   // shared tiles and scan storage are reused
+    }
+}
+
+// inserted pairs (insert_idea2, src/scc_incremental.cc:18-27) mapped through
+// the labels and appended when they join two SCCs
+__global__ void k_cond_batch(int64_t k, const int32_t* __restrict__ a, const int32_t* __restrict__ b,
+                             const int32_t* __restrict__ label, int32_t n, int32_t* __restrict__ out_src,
+                             int32_t* __restrict__ out_dst, int32_t* __restrict__ count, int* __restrict__ bad) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < k; i += (int64_t)gridDim.x * blockDim.x) {
         int32_t x = a[i], y = b[i];
-        if (x < 0 || x >= n || y < 0 || y >= n) { atomicExch(bad, 1); src[i] = dst[i] = 0; continue; }
-        src[i] = label[x];
-        dst[i] = label[y];
+        if (x < 0 || x >= n || y < 0 || y >= n) { atomicExch(bad, 1); continue; }
+        int32_t lx = label[x], ly = label[y];
+        if (lx == ly) continue;
+        int32_t at = atomicAdd(count, 1);
+        out_src[at] = lx;
+        out_dst[at] = ly;
     }
-}
-
-// 1 where an edge joins two different SCCs (the only edges the condensation keeps)
-__global__ void k_cond_flags(int64_t m, const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
-                             uint8_t* __restrict__ flags) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
-        flags[i] = src[i] != dst[i];
 }
 
 extern "C" int scc_condensation_graph(const scc_graph* g, const int32_t* labels, int32_t num_sccs, int64_t n_ins,
                                       const int32_t* ins_src, const int32_t* ins_dst, scc_graph** out) {
     SCC_REQUIRE(g && labels && out && num_sccs >= 0, SCC_ERR_INVALID, "NULL argument");
     SCC_REQUIRE(n_ins == 0 || (ins_src && ins_dst), SCC_ERR_INVALID, "NULL batch arrays");
+    SCC_REQUIRE(n_ins >= 0 && g->m + n_ins < (1LL << 31) - 1, SCC_ERR_INVALID, "batch of %lld edges too large",
+                (long long)n_ins);
     SCC_CUDA(cudaSetDevice(g->device));
     cudaStream_t st;
     SCC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    int64_t total = g->m + n_ins;
+    const int64_t total = g->m + n_ins;
+    const int64_t chunks = (g->m + COND_CHUNK - 1) / COND_CHUNK;
     int rc = SCC_OK;
     {   // buffers are freed on `st` before it is destroyed
-    DevBuf lab, src, dst, bs, bd, bad;
+    DevBuf lab, osrc, odst, own, bs, bd, ctr;
     if ((rc = alloc(lab, sizeof(int32_t) * (size_t)g->n, st)) == SCC_OK &&
-        (rc = alloc(src, sizeof(int32_t) * (size_t)total, st)) == SCC_OK &&
-        (rc = alloc(dst, sizeof(int32_t) * (size_t)total, st)) == SCC_OK &&
+        (rc = alloc(osrc, sizeof(int32_t) * (size_t)total, st)) == SCC_OK &&
+        (rc = alloc(odst, sizeof(int32_t) * (size_t)total, st)) == SCC_OK &&
+        (rc = alloc(own, sizeof(int32_t) * (size_t)(chunks + 1), st)) == SCC_OK &&
         (rc = alloc(bs, sizeof(int32_t) * (size_t)n_ins, st)) == SCC_OK &&
-        (rc = alloc(bd, sizeof(int32_t) * (size_t)n_ins, st)) == SCC_OK && (rc = alloc(bad, sizeof(int), st)) == SCC_OK) {
-        cudaMemsetAsync(bad.p, 0, sizeof(int), st);
+        (rc = alloc(bd, sizeof(int32_t) * (size_t)n_ins, st)) == SCC_OK &&
+        (rc = alloc(ctr, 2 * sizeof(int), st)) == SCC_OK) {
+        int* bad = ctr.as<int>();
+        int32_t* count = ctr.as<int32_t>() + 1;
+        cudaMemsetAsync(ctr.p, 0, 2 * sizeof(int), st);
         cudaMemcpyAsync(lab.p, labels, sizeof(int32_t) * (size_t)g->n, cudaMemcpyHostToDevice, st);
         if (g->n > 0)
-            k_cond_map<<<scc_blocks((int64_t)g->n * 32, SCC_THREADS, 148 * 16), SCC_THREADS, 0, st>>>(
-                g->n, g->begin, g->node_idx, lab.as<int32_t>(), num_sccs, src.as<int32_t>(), dst.as<int32_t>(),
-                bad.as<int>());
+            k_cond_check_labels<<<scc_blocks(g->n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, st>>>(
+                g->n, lab.as<int32_t>(), num_sccs, bad);
+        if (g->m > 0) {
+            k_cond_owners<<<scc_blocks(chunks + 1), SCC_THREADS, 0, st>>>(g->n, chunks, g->begin, own.as<int32_t>());
+            // one resident wave: a grid-stride loop over chunks with a second
+            // wave would leave its blocks a full share of chunks to run late
+            int sms = 148, per = 1;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cond_cross, SCC_THREADS, 0);
+            k_cond_cross<<<(unsigned)std::min<int64_t>(chunks, (int64_t)sms * std::max(per, 1)), SCC_THREADS, 0, st>>>(
+                (int32_t)g->m, chunks, g->begin, g->node_idx, lab.as<int32_t>(), own.as<int32_t>(),
+                osrc.as<int32_t>(), odst.as<int32_t>(), count);
+        }
         if (n_ins > 0) {
             cudaMemcpyAsync(bs.p, ins_src, sizeof(int32_t) * (size_t)n_ins, cudaMemcpyHostToDevice, st);
             cudaMemcpyAsync(bd.p, ins_dst, sizeof(int32_t) * (size_t)n_ins, cudaMemcpyHostToDevice, st);
-            k_cond_map_batch<<<scc_blocks(n_ins), SCC_THREADS, 0, st>>>(n_ins, bs.as<int32_t>(), bd.as<int32_t>(),
-                                                                        lab.as<int32_t>(), g->n,
-                                                                        src.as<int32_t>() + g->m,
-                                                                        dst.as<int32_t>() + g->m, bad.as<int>());
+            k_cond_batch<<<scc_blocks(n_ins), SCC_THREADS, 0, st>>>(n_ins, bs.as<int32_t>(), bd.as<int32_t>(),
+                                                                    lab.as<int32_t>(), g->n, osrc.as<int32_t>(),
+                                                                    odst.as<int32_t>(), count, bad);
         }
-        int hbad = 0;
-        cudaError_t e = cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+        int h[2] = {0, 0};
+        cudaError_t e = cudaPeekAtLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h, ctr.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = scc_cuda_status(e, "condensation map", __FILE__, __LINE__);
-        else if (hbad) { scc_set_error("label or inserted endpoint out of range"); rc = SCC_ERR_INVALID; }
-        else {
-            // intra-SCC pairs would become self-loops the build drops: compact
-            // the cross-SCC pairs first, so the build sorts only those
-            DevBuf flags, src2, dst2, num, tmp;
-            size_t tb = 0;
-            if ((rc = alloc(flags, (size_t)total, st)) == SCC_OK &&
-                (rc = alloc(src2, sizeof(int32_t) * (size_t)total, st)) == SCC_OK &&
-                (rc = alloc(dst2, sizeof(int32_t) * (size_t)total, st)) == SCC_OK &&
-                (rc = alloc(num, sizeof(int32_t), st)) == SCC_OK) {
-                int32_t hnum = 0;
-                k_cond_flags<<<scc_blocks(total, SCC_THREADS, 148 * 16), SCC_THREADS, 0, st>>>(
-                    total, src.as<int32_t>(), dst.as<int32_t>(), flags.as<uint8_t>());
-                e = cudaPeekAtLastError();
-                if (e == cudaSuccess)
-                    e = cub::DeviceSelect::Flagged(nullptr, tb, src.as<int32_t>(), flags.as<uint8_t>(), src2.as<int32_t>(),
-                                                   num.as<int32_t>(), (int)total, st);
-                if (e == cudaSuccess && (rc = alloc(tmp, tb, st)) == SCC_OK) {
-                    e = cub::DeviceSelect::Flagged(tmp.p, tb, src.as<int32_t>(), flags.as<uint8_t>(), src2.as<int32_t>(),
-                                                   num.as<int32_t>(), (int)total, st);
-                    if (e == cudaSuccess)
-                        e = cub::DeviceSelect::Flagged(tmp.p, tb, dst.as<int32_t>(), flags.as<uint8_t>(),
-                                                       dst2.as<int32_t>(), num.as<int32_t>(), (int)total, st);
-                    if (e == cudaSuccess) e = cudaMemcpyAsync(&hnum, num.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
-                    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-                    if (e != cudaSuccess) rc = scc_cuda_status(e, "condensation compaction", __FILE__, __LINE__);
-                    else rc = scc_impl_build_graph_from_device_edges(num_sccs, hnum, src2.as<int32_t>(), dst2.as<int32_t>(),
-                                                                      SCC_BUILD_DEDUP | SCC_BUILD_NO_SELF_LOOPS,
-                                                                      g->device, out);
-                } else if (e != cudaSuccess) {
-                    rc = scc_cuda_status(e, "condensation compaction", __FILE__, __LINE__);
-                }
-            }
-        }
+        else if (h[0]) { scc_set_error("label or inserted endpoint out of range"); rc = SCC_ERR_INVALID; }
+        else rc = scc_impl_build_graph_from_device_edges(num_sccs, h[1], osrc.as<int32_t>(), odst.as<int32_t>(),
+                                                         SCC_BUILD_DEDUP | SCC_BUILD_NO_SELF_LOOPS, g->device, out);
     }
     }
     cudaStreamSynchronize(st);

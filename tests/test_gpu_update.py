@@ -115,6 +115,38 @@ def test_insert_idea1_recomputes(gpu):
     check(g, st, n, *apply_batch(s, d, ins_s, ins_d, [], []))
 
 
+def test_condensation_graph_chunk_layout(gpu):
+    # the cross-pair kernel works in 2,048-edge chunks: a hub spanning many
+    # chunks, isolated runs wider than a chunk's vertex tile (in the middle
+    # and at the end), and an edge count off every chunk boundary
+    rng = np.random.default_rng(11)
+    n = 60000
+    parts = [(np.full(50001, 5), rng.integers(0, n, 50001)),
+             (rng.integers(0, 20000, 30000), rng.integers(0, n, 30000)),
+             (rng.integers(40000, 55000, 7777), rng.integers(0, n, 7777)),
+             (np.arange(20000, 20003), np.arange(40000, 40003))]
+    s = np.concatenate([p[0] for p in parts]).astype(np.int32)
+    d = np.concatenate([p[1] for p in parts]).astype(np.int32)
+    k = 3000
+    ids = rng.integers(0, k, n).astype(np.int32)   # any grouping, not only SCCs
+    ins_s = rng.integers(0, n, 64).astype(np.int32); ins_d = rng.integers(0, n, 64).astype(np.int32)
+    g = Graph.from_edges(n, s, d)
+    for bs, bd in (((), ()), (ins_s, ins_d)):
+        c = condensation_graph(g, ids, k, bs, bd)
+        ms = np.concatenate([ids[s], ids[np.asarray(bs, np.int32)]])
+        md = np.concatenate([ids[d], ids[np.asarray(bd, np.int32)]])
+        keep = ms != md
+        exp_s, exp_d = O.dedup_edges(ms[keep], md[keep], n=k)
+        cb, ca, rb, ra = c.csr()
+        assert np.array_equal(np.repeat(np.arange(k, dtype=np.int32), np.diff(cb)), exp_s)
+        assert np.array_equal(ca, exp_d)
+        order = np.lexsort((exp_s, exp_d))
+        assert np.array_equal(np.repeat(np.arange(k, dtype=np.int32), np.diff(rb)), exp_d[order])
+        assert np.array_equal(ra, exp_s[order])
+        c.free()
+    g.free()
+
+
 def test_condensation_graph(gpu):
     n = 800
     s, d = random_graph(n, 1500, 5)
