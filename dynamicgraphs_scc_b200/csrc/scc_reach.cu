@@ -460,6 +460,10 @@ __global__ void __launch_bounds__(ASYNC_THREADS, 1) k_reach_async(RoundArgs a, i
     long long my_items = 0;     // warp-uniform
     while (true) {
         if (push.count == 0) {
+            // publish this warp's net change to the outstanding work before it
+            // waits: the count reaches zero only once every warp has done so
+            if (lane == 0 && push.pushed != 0) atomicAdd(work, push.pushed);
+            push.pushed = 0;
             int32_t got = 0, base = 0;
             if (lane == 0) {
                 int32_t t = ld_volatile(tail), h = ld_volatile(head);
@@ -517,24 +521,26 @@ __global__ void __launch_bounds__(ASYNC_THREADS, 1) k_reach_async(RoundArgs a, i
         push.count -= k;
         expand_warp_async(a, lane < k, it, ib, ie, ix0, ix1, ix2, push, &my_edges);
         my_items += k;
-        int32_t delta = push.pushed - k;
-        push.pushed = 0;
+        // the net change (pushed - expanded) accumulates in push.pushed and is
+        // published every 8th iteration, before a spill makes items visible,
+        // and before the warp waits: one counter update per 8 iterations
+        // instead of one per iteration, on a line every idle warp polls
+        push.pushed -= k;
         if ((++iter & 7) == 0) {
-            // every 8th iteration: read back the outstanding work; a frontier that
-            // has grown wide is handed back to the level-synchronous kernels,
-            // which expand wide frontiers far better than one queue
+            // read back the outstanding work; a frontier that has grown wide is
+            // handed back to the level-synchronous kernels, which expand wide
+            // frontiers far better than one queue
             int32_t stop = 0;
             if (lane == 0) {
-                int32_t w = atomicAdd(work, delta) + delta;
+                int32_t w = atomicAdd(work, push.pushed) + push.pushed;
                 if (w > a.async_bail) atomicExch(bail, 1);
                 stop = ld_volatile(bail);
             }
+            push.pushed = 0;
             if (__shfl_sync(0xFFFFFFFFu, stop, 0)) {
                 push.spill(0);
                 break;
             }
-        } else if (lane == 0 && delta != 0) {
-            atomicAdd(work, delta);
         }
         // keep one iteration's worth (this warp's own continuation), share the rest
         if (push.count > push.keep) push.spill(push.keep);
