@@ -64,11 +64,11 @@ WORKLOAD_NAMES = {
 
 # DRAM traffic of the asynchronous drain relative to its algorithmic bytes,
 # from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum over all
-# launches) of `bench.py --workload grid4096 --steps 1 --warmup 0`: 579.97 MB
-# read + written by 9 launches whose algorithmic bytes total 791.2 MB.  The
+# launches) of `bench.py --workload grid4096 --steps 1 --warmup 0`: 595.40 MB
+# read + written by 9 launches whose algorithmic bytes total 793.8 MB.  The
 # full C2 step is too large for that capture; its drain runs the same grid.
-ASYNC_TRAFFIC_RATIO = 579.97 / 791.2
-ASYNC_TRAFFIC_SOURCE = "ncu dram bytes on the 4096x4096 grid workload (0.733 x algorithmic), scaled per launch"
+ASYNC_TRAFFIC_RATIO = 595.40 / 793.8
+ASYNC_TRAFFIC_SOURCE = "ncu dram bytes on the 4096x4096 grid workload (0.750 x algorithmic), scaled per launch"
 
 
 def measured_peak_gbs():
