@@ -14,8 +14,15 @@
 // direction, visited bits in a byte per vertex), and a classify pass gives
 // each class the reference's outcome.  A single class (curr_color) is the
 // global step.
+#include <time.h>
 #include <algorithm>
 #include "scc_round.cuh"
+
+static double trace_ms() {
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return t.tv_sec * 1e3 + t.tv_nsec * 1e-6;
+}
 
 // Reset the per-colour pivot slots of the classes present and total the
 // in+out degree of the vertices this round will traverse (the direction rule
@@ -256,6 +263,7 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
 // per round, so the loop ends.
 int scc_impl_resolve_all(const scc_graph* g, scc_state* s, bool classes_split) {
     if (s->live_count < 0) SCC_TRY(scc_impl_compact_live(g, s, true));
+    double t_round = scc_trace_on() ? trace_ms() : 0.0;
     for (int round = 0; round < (1 << 30); ++round) {
         int32_t t = 0;
         SCC_TRY(scc_impl_trim1(g, s, true, &t));
@@ -269,9 +277,12 @@ int scc_impl_resolve_all(const scc_graph* g, scc_state* s, bool classes_split) {
         SCC_TRY(scc_impl_fb_round(g, s, INT32_MIN, -1, &found, &act, true));
         SCC_TRY(scc_impl_compact_live(g, s, false));   // synchronises: classify's count is current
         found = s->h_ctr[CTR_COUNT];
-        if (scc_trace_on())
-            fprintf(stderr, "[scc] round %d: trimmed=%d live=%d classes=%d scc_found=%d left=%d\n", round, t,
-                    live_before, classes, found, s->live_count);
+        if (scc_trace_on()) {
+            double t1 = trace_ms();
+            fprintf(stderr, "[scc] round %d: trimmed=%d live=%d classes=%d scc_found=%d left=%d %.3f ms\n", round, t,
+                    live_before, classes, found, s->live_count, t1 - t_round);
+            t_round = t1;
+        }
         s->fb_rounds++;
         if (s->live_count == 0) break;
         if (found == 0) { scc_set_error("FW-BW round made no progress"); return SCC_ERR_STATE; }
