@@ -99,6 +99,7 @@ struct scc_state {
     int32_t* aq = nullptr;           // [2n+64] asynchronous traversal queue, kept at -1 between uses
     int32_t* uf = nullptr;           // [n] union-find parents (weak-component split)
     unsigned long long* cnt = nullptr;   // [n] live counts of the counting peel, (in << 32) | out; also n ints of scratch for updates
+    unsigned long long* ccnt = nullptr;  // [n] counts within colours of later peels (allocated at first use)
     int32_t* hq = nullptr;           // [2n+64] high-degree items deferred by a top-down level
     long long* hoff = nullptr;       // [2n+64] prefix of their degrees
     uint8_t* mark = nullptr;         // [n rounded to 4] reachability marks (bit0 FW, bit1 BW)

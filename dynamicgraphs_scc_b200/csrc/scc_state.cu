@@ -222,7 +222,7 @@ extern "C" int scc_state_free(scc_state* s) {
     if (!s) return SCC_OK;
     cudaSetDevice(s->device);
     cudaFree(s->color); cudaFree(s->scc); cudaFree(s->wcc); cudaFree(s->live); cudaFree(s->live_tmp);
-    cudaFree(s->qa); cudaFree(s->qb); cudaFree(s->aq); cudaFree(s->uf); cudaFree(s->hq); cudaFree(s->hoff); cudaFree(s->cnt); cudaFree(s->mark); cudaFree(s->aux); cudaFree(s->block_sums);
+    cudaFree(s->qa); cudaFree(s->qb); cudaFree(s->aq); cudaFree(s->uf); cudaFree(s->hq); cudaFree(s->hoff); cudaFree(s->cnt); cudaFree(s->ccnt); cudaFree(s->mark); cudaFree(s->aux); cudaFree(s->block_sums);
     cudaFree(s->ctr);
     if (s->h_ctr) cudaFreeHost(s->h_ctr);
     cudaFree(s->slot_key); cudaFree(s->slot_pivot); cudaFree(s->slot_fw); cudaFree(s->slot_bw); cudaFree(s->slot_count);

@@ -16,6 +16,7 @@
 // only live out-neighbour (ignoring self-loops and repeats) is k and k's is n,
 // or the same on in-edges, is a 2-vertex SCC with scc = n.  Decisions are
 // taken on the colours before the pass (a find kernel, then an apply kernel).
+#include <algorithm>
 #include "scc_internal.cuh"
 
 #define TRIM_STACK 8
@@ -243,6 +244,7 @@ struct CountArgs {
     int32_t* color; int32_t* scc; unsigned long long* cnt;
     int32_t* ovf; int32_t* ctr;
     int32_t* hub;           // trimmed vertices above PEEL_HUB edges, expanded edge-parallel (count CTR_SPARE3)
+    const int32_t* snap;    // coloured peel: the colours before it (a trimmed vertex's class); else unused
 };
 
 #define PEEL_Q 256          // per-warp queue of trimmed vertices awaiting expansion
@@ -250,19 +252,22 @@ struct CountArgs {
 #define CNT_IN_ONE (1ull << 32)
 
 // One edge of trimmed x: out-edges take an in-neighbour from w, in-edges an
-// out-neighbour; returns the neighbour this decrement trims, or -1.
+// out-neighbour; returns the neighbour this decrement trims, or -1.  COL: the
+// counts are within colours, so only a neighbour still in x's class (cx) is
+// decremented -- exactly the edges its count included.
+template <bool COL>
 __device__ __forceinline__ int32_t peel_edge(const CountArgs& a, int32_t x, int32_t ob, int32_t od, int32_t ib,
-                                             int32_t k) {
+                                             int32_t k, int32_t cx) {
     int32_t nv = -1;
     if (k < od) {
         int32_t w = __ldg(a.node_idx + ob + k);
-        if (w != x) {
+        if (w != x && (!COL || ld_cg(a.color + w) == cx)) {
             unsigned long long old = atomicAdd(a.cnt + w, 0ull - CNT_IN_ONE);
             if ((old >> 32) == 1ull && (uint32_t)old != 0u) nv = w;
         }
     } else {
         int32_t u = __ldg(a.r_node_idx + ib + (k - od));
-        if (u != x) {
+        if (u != x && (!COL || ld_cg(a.color + u) == cx)) {
             unsigned long long old = atomicAdd(a.cnt + u, 0ull - 1ull);
             if ((uint32_t)old == 1u && (old >> 32) != 0ull) nv = u;
         }
@@ -281,6 +286,7 @@ __device__ __forceinline__ int32_t peel_edge(const CountArgs& a, int32_t x, int3
 // in-neighbours an out-neighbour -- so a warp issues 32 independent atomics
 // per round trip.  The atomic that zeroes the first half of a word trims that
 // neighbour, which joins the queue, or the overflow list when the queue is full.
+template <bool COL>
 __device__ void peel_drain(const CountArgs& a, int32_t* wq, int32_t& qn, int32_t& cnt) {
     const int lane = threadIdx.x & 31;
     const unsigned full = 0xFFFFFFFFu;
@@ -289,8 +295,9 @@ __device__ void peel_drain(const CountArgs& a, int32_t* wq, int32_t& qn, int32_t
         qn -= take;
         const int32_t x = lane < take ? wq[qn + lane] : -1;
         __syncwarp();
-        int32_t ob = 0, od = 0, ib = 0, id = 0;
+        int32_t ob = 0, od = 0, ib = 0, id = 0, cx = 0;
         if (x >= 0) {
+            if (COL) cx = a.snap[x];
             ob = __ldg(a.begin + x); od = __ldg(a.begin + x + 1) - ob;
             ib = __ldg(a.r_begin + x); id = __ldg(a.r_begin + x + 1) - ib;
             if (od + id > PEEL_HUB) {
@@ -320,8 +327,9 @@ __device__ void peel_drain(const CountArgs& a, int32_t* wq, int32_t& qn, int32_t
             const int32_t ox = __shfl_sync(full, x, owner);
             const int32_t oob = __shfl_sync(full, ob, owner), ood = __shfl_sync(full, od, owner);
             const int32_t oib = __shfl_sync(full, ib, owner);
+            const int32_t ocx = COL ? __shfl_sync(full, cx, owner) : 0;
             int32_t nv = -1;
-            if (j < total) nv = peel_edge(a, ox, oob, ood, oib, k);
+            if (j < total) nv = peel_edge<COL>(a, ox, oob, ood, oib, k, ocx);
             const unsigned bal = __ballot_sync(full, nv >= 0);
             if (bal) {
                 const int32_t r = __popc(bal & ((1u << lane) - 1u)), nn = __popc(bal);
@@ -342,9 +350,12 @@ __device__ void peel_drain(const CountArgs& a, int32_t* wq, int32_t& qn, int32_t
 }
 
 // Sweep (items == NULL): every seed is trimmed and expanded.  List (items !=
-// NULL): expand trimmed vertices that overflowed a queue.  Each warp drains
-// its queue after every 32 vertices.
-__global__ void __launch_bounds__(SCC_THREADS) k_count_peel(CountArgs a, int32_t n, const int32_t* __restrict__ items) {
+// NULL): expand trimmed vertices that overflowed a queue, or, with
+// trim_items, trim the listed seeds of a coloured peel and expand them.  Each
+// warp drains its queue after every 32 vertices.
+template <bool COL>
+__global__ void __launch_bounds__(SCC_THREADS) k_count_peel(CountArgs a, int32_t n, const int32_t* __restrict__ items,
+                                                            int trim_items) {
     __shared__ int32_t queues[SCC_THREADS / 32][PEEL_Q];
     const int lane = threadIdx.x & 31;
     int32_t* wq = queues[threadIdx.x >> 5];
@@ -356,6 +367,11 @@ __global__ void __launch_bounds__(SCC_THREADS) k_count_peel(CountArgs a, int32_t
         if (i < n) {
             if (items) {
                 x = items[i];
+                if (trim_items) {
+                    a.color[x] = SCC_COLOR_DONE;
+                    a.scc[x] = x;
+                    cnt++;
+                }
             } else {
                 // only the sweep writes a seed's colour, so a plain read decides
                 int32_t v = (int32_t)i;
@@ -375,7 +391,7 @@ __global__ void __launch_bounds__(SCC_THREADS) k_count_peel(CountArgs a, int32_t
         if (x >= 0) wq[qn + __popc(bal & ((1u << lane) - 1u))] = x;    // qn == 0 here
         qn += __popc(bal);
         __syncwarp();
-        peel_drain(a, wq, qn, cnt);
+        peel_drain<COL>(a, wq, qn, cnt);
     }
     block_count_add(a.ctr + CTR_COUNT, cnt);
 }
@@ -411,6 +427,7 @@ __global__ void k_hub_prefix(const int32_t* __restrict__ begin, const int32_t* _
 // Edge-parallel expansion of trimmed hubs: thread t takes edge t of their
 // concatenated lists; trims it causes go to the overflow list, expanded by the
 // next list launch of k_count_peel.
+template <bool COL>
 __global__ void k_hub_peel(CountArgs a, const int32_t* __restrict__ hubs, int32_t cnt,
                            const long long* __restrict__ hoff) {
     const long long total = hoff[cnt - 1];
@@ -425,7 +442,7 @@ __global__ void k_hub_peel(CountArgs a, const int32_t* __restrict__ hubs, int32_
             const int32_t x = hubs[lo];
             const long long start = lo ? hoff[lo - 1] : 0;
             const int32_t ob = __ldg(a.begin + x), od = __ldg(a.begin + x + 1) - ob, ib = __ldg(a.r_begin + x);
-            nv = peel_edge(a, x, ob, od, ib, (int32_t)(t - start));
+            nv = peel_edge<COL>(a, x, ob, od, ib, (int32_t)(t - start), COL ? a.snap[x] : 0);
         }
         const unsigned bal = __ballot_sync(0xFFFFFFFFu, nv >= 0);
         if (bal) {
@@ -445,7 +462,7 @@ static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     CountArgs a;
     a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin; a.r_node_idx = g->r_node_idx;
     a.color = s->color; a.scc = s->scc; a.cnt = s->cnt;
-    a.ovf = s->qa; a.ctr = s->ctr; a.hub = s->hq;
+    a.ovf = s->qa; a.ctr = s->ctr; a.hub = s->hq; a.snap = nullptr;
     SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
     SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
     SCC_TRY(scc_zero_counters(s, CTR_SPARE3, 1));
@@ -454,7 +471,7 @@ static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
                                                                g->self_loops > 0 ? 1 : 0, s->cnt, s->color,
                                                                s->prefinished ? 1 : 0);
     SCC_LAUNCHED(s);
-    k_count_peel<<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, n, nullptr);
+    k_count_peel<false><<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, n, nullptr, 0);
     SCC_LAUNCHED(s);
     int64_t total = 0;
     // Rounds: overflowed trims are expanded by a list launch, hubs edge-parallel
@@ -476,11 +493,11 @@ static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
         if (nhub > 0) {
             k_hub_prefix<<<1, 1024, 0, s->stream>>>(g->begin, g->r_begin, s->aux, nhub, s->hoff);
             SCC_LAUNCHED(s);
-            k_hub_peel<<<148 * 8, SCC_THREADS, 0, s->stream>>>(a, s->aux, nhub, s->hoff);
+            k_hub_peel<false><<<148 * 8, SCC_THREADS, 0, s->stream>>>(a, s->aux, nhub, s->hoff);
             SCC_LAUNCHED(s);
         }
         if (novf > 0) {
-            k_count_peel<<<scc_blocks(novf, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, novf, s->qb);
+            k_count_peel<false><<<scc_blocks(novf, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, novf, s->qb, 0);
             SCC_LAUNCHED(s);
         }
     }
@@ -488,6 +505,128 @@ static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     s->cnt_valid = !s->prefinished;      // the residue of finished vertices is not a count
     s->fresh = false;
     s->prefinished = false;
+    s->prefinished = false;
+    return SCC_OK;
+}
+
+// ---------------------------------------------------------------- coloured counting peel
+// Later peels run inside colours over the live list.  The scanning sweep
+// re-reads a neighbour's lists at every trim next to it, and its cascades run
+// in single threads (a grid's chains of trimmable vertices left 3 lanes of 32
+// busy).  Instead, count each live vertex's same-colour in- and out-
+// neighbours once, list the vertices with a zero count, and peel with the warp
+// queues of the first peel, decrementing only neighbours still in the trimmed
+// vertex's class (its colour before the peel is in the snapshot).  The set
+// peeled is the same unique fixpoint.
+#define CCOUNT_WARP_DEG 64   // a live vertex with more edges is counted by its whole warp
+#define CCOUNT_MIN_LIVE 32768   // smaller live lists: one scanning sweep costs less than the extra round trip
+
+__global__ void k_ccount_init(CountArgs a, const int32_t* __restrict__ live, int32_t n_items,
+                              int32_t* __restrict__ seeds, int32_t* __restrict__ nseeds) {
+    const unsigned full = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < n_items;
+         base += nwarps * 32) {
+        const int64_t i = base + lane;
+        int32_t v = 0, c = SCC_COLOR_DONE, ob = 0, oe = 0, ib = 0, ie = 0;
+        if (i < n_items) {
+            v = live[i];
+            c = a.color[v];
+            if (c != SCC_COLOR_DONE) {
+                ob = __ldg(a.begin + v); oe = __ldg(a.begin + v + 1);
+                ib = __ldg(a.r_begin + v); ie = __ldg(a.r_begin + v + 1);
+            }
+        }
+        const bool on = c != SCC_COLOR_DONE;
+        const bool wide = on && (oe - ob) + (ie - ib) > CCOUNT_WARP_DEG;
+        uint32_t co = 0, ci = 0;
+        if (on && !wide) {
+            for (int32_t k = ob; k < oe; ++k) { int32_t w = __ldg(a.node_idx + k); co += (w != v && a.color[w] == c); }
+            for (int32_t k = ib; k < ie; ++k) { int32_t u = __ldg(a.r_node_idx + k); ci += (u != v && a.color[u] == c); }
+        }
+        unsigned wm = __ballot_sync(full, wide);
+        while (wm) {
+            const int l = __ffs(wm) - 1;
+            wm &= wm - 1;
+            const int32_t lv = __shfl_sync(full, v, l), lc = __shfl_sync(full, c, l);
+            const int32_t lob = __shfl_sync(full, ob, l), loe = __shfl_sync(full, oe, l);
+            const int32_t lib = __shfl_sync(full, ib, l), lie = __shfl_sync(full, ie, l);
+            uint32_t so = 0, si = 0;
+            for (int32_t k = lob + lane; k < loe; k += 32) { int32_t w = __ldg(a.node_idx + k); so += (w != lv && a.color[w] == lc); }
+            for (int32_t k = lib + lane; k < lie; k += 32) { int32_t u = __ldg(a.r_node_idx + k); si += (u != lv && a.color[u] == lc); }
+            so = __reduce_add_sync(full, so);
+            si = __reduce_add_sync(full, si);
+            if (lane == l) { co = so; ci = si; }
+        }
+        const bool seed = on && (co == 0 || ci == 0);
+        if (on) a.cnt[v] = ((unsigned long long)ci << 32) | co;
+        const unsigned sb = __ballot_sync(full, seed);
+        if (sb) {
+            int32_t at = 0;
+            if (lane == 0) at = atomicAdd(nseeds, __popc(sb));
+            at = __shfl_sync(full, at, 0);
+            if (seed) seeds[at + __popc(sb & ((1u << lane) - 1u))] = v;
+        }
+    }
+}
+
+// Buffers: seeds in qb (read by the first peel launch only), overflow in qa
+// (copied to qb for each list launch), hubs in hq (copied to live_tmp), class
+// snapshot in aux, counts in the state's own coloured-count array.
+__global__ void k_copy_list_i32(const int32_t* __restrict__ list, int64_t n, const int32_t* __restrict__ a,
+                                int32_t* __restrict__ b);
+
+static int trim1_coloured(const scc_graph* g, scc_state* s, int32_t* trimmed) {
+    const int32_t n_items = s->live_count;
+    if (!s->ccnt) SCC_CUDA(cudaMalloc(&s->ccnt, sizeof(unsigned long long) * (size_t)std::max<int32_t>(g->n, 1)));
+    CountArgs a;
+    a.begin = g->begin; a.node_idx = g->node_idx; a.r_begin = g->r_begin; a.r_node_idx = g->r_node_idx;
+    a.color = s->color; a.scc = s->scc; a.cnt = s->ccnt;
+    a.ovf = s->qa; a.ctr = s->ctr; a.hub = s->hq; a.snap = s->aux;
+    k_copy_list_i32<<<scc_blocks(n_items), SCC_THREADS, 0, s->stream>>>(s->live, n_items, s->color, s->aux);
+    SCC_LAUNCHED(s);
+    SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
+    SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
+    SCC_TRY(scc_zero_counters(s, CTR_SPARE3, 1));
+    SCC_TRY(scc_zero_counters(s, CTR_QLEN, 1));
+    k_ccount_init<<<scc_blocks(n_items, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(
+        a, s->live, n_items, s->qb, s->ctr + CTR_QLEN);
+    SCC_LAUNCHED(s);
+    SCC_TRY(scc_sync_counters(s));
+    const int32_t nseeds = s->h_ctr[CTR_QLEN];
+    int64_t total = 0;
+    if (nseeds > 0) {
+        k_count_peel<true><<<scc_blocks(nseeds, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, nseeds, s->qb, 1);
+        SCC_LAUNCHED(s);
+        for (int round = 0; round < 1000000; ++round) {
+            SCC_TRY(scc_sync_counters(s));
+            total += s->h_ctr[CTR_COUNT];
+            int32_t novf = s->h_ctr[CTR_OVERFLOW];
+            int32_t nhub = s->h_ctr[CTR_SPARE3];
+            if (novf == 0 && nhub == 0) break;
+            SCC_TRY(scc_zero_counters(s, CTR_COUNT, 1));
+            if (novf > 0)
+                SCC_CUDA(cudaMemcpyAsync(s->qb, s->qa, sizeof(int32_t) * (size_t)novf, cudaMemcpyDeviceToDevice, s->stream));
+            if (nhub > 0)
+                SCC_CUDA(cudaMemcpyAsync(s->live_tmp, s->hq, sizeof(int32_t) * (size_t)nhub, cudaMemcpyDeviceToDevice,
+                                         s->stream));
+            SCC_TRY(scc_zero_counters(s, CTR_OVERFLOW, 1));
+            SCC_TRY(scc_zero_counters(s, CTR_SPARE3, 1));
+            if (nhub > 0) {
+                k_hub_prefix<<<1, 1024, 0, s->stream>>>(g->begin, g->r_begin, s->live_tmp, nhub, s->hoff);
+                SCC_LAUNCHED(s);
+                k_hub_peel<true><<<148 * 8, SCC_THREADS, 0, s->stream>>>(a, s->live_tmp, nhub, s->hoff);
+                SCC_LAUNCHED(s);
+            }
+            if (novf > 0) {
+                k_count_peel<true><<<scc_blocks(novf, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, novf, s->qb, 0);
+                SCC_LAUNCHED(s);
+            }
+        }
+    }
+    *trimmed = (int32_t)total;
+    s->fresh = false;
     s->prefinished = false;
     return SCC_OK;
 }
@@ -602,6 +741,7 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
     if (n_items <= 0) return SCC_OK;
     // snapshot colours (aux) so overflowed vertices keep their pre-trim colour
     if ((s->fresh || s->prefinished) && !use_live && s->cnt) return trim1_counting(g, s, trimmed);
+    if (use_live && n_items >= CCOUNT_MIN_LIVE) return trim1_coloured(g, s, trimmed);
     s->prefinished = false;
     bool fresh = s->fresh && !use_live;
     if (fresh) {

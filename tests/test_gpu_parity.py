@@ -93,6 +93,37 @@ def test_trim1_respects_colours(gpu):
     assert t == ot and np.array_equal(st.color(), oc)
 
 
+@pytest.mark.parametrize("seed", [3, 4])
+def test_trim1_on_live_list_within_colours(gpu, seed):
+    # a long live list (>= 32,768 vertices) is peeled by counting neighbours
+    # inside colours once and expanding trims from warp queues: the same
+    # fixpoint as the oracle's scanning peel, with finished vertices, several
+    # colours, duplicate and self-loop edges, and a 10,000-edge hub that is a
+    # seed (no in-edges) and is expanded edge-parallel
+    n0, s, d, _ = seeded_graph(rmat_scale=16, edge_factor=4, grid_side=256, seed=seed)
+    rng = np.random.default_rng(seed)
+    hub = n0
+    n = n0 + 1
+    s = np.concatenate([s, np.full(10000, hub, np.int32), rng.integers(0, n0, 3000).astype(np.int32)])
+    d = np.concatenate([d, rng.integers(0, n0, 10000).astype(np.int32), rng.integers(0, n0, 3000).astype(np.int32)])
+    s = np.concatenate([s, s[:500]]); d = np.concatenate([d, d[:500]])          # duplicates
+    s = np.concatenate([s, np.arange(0, 200, dtype=np.int32)]); d = np.concatenate([d, np.arange(0, 200, dtype=np.int32)])
+    csr = O.build_csr(n, s, d)
+    color = rng.integers(-2, 3, n).astype(np.int32)
+    color[hub] = 0
+    scc = np.where(color == -2, np.arange(n, dtype=np.int32), -1).astype(np.int32)
+    g = Graph.from_edges(n, s, d)
+    st = State(g)
+    st.set_color(color); st.set_scc(scc)
+    assert st.create_trim1_compact() >= 32768
+    t = st.repeat_global_trim1_compact()
+    oc = color.copy(); os_ = scc.copy()
+    ot = O.trim1_fixpoint(csr, oc, os_)
+    assert t == ot and t > 0
+    assert np.array_equal(st.color(), oc)
+    assert np.array_equal(st.scc(), os_)
+
+
 def test_global_fw_bw_exact(gpu):
     n, s, d, csr = seeded_graph(rmat_scale=14, edge_factor=8, seed=17)
     g = Graph.from_edges(n, s, d)
