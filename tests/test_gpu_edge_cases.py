@@ -28,6 +28,28 @@ def _check(n, s, d):
     st.free(); g.free()
 
 
+def test_weak_split_on_a_million_live_vertices(gpu):
+    # after the global step more than 2^20 vertices stay live: an oriented
+    # 1024 x 1024 grid (one giant weak component of many SCCs) beside 120,000
+    # disjoint 3-cycles, all split by one union-find pass over the live list
+    from tests.helpers import seeded_graph
+    n0, s, d, _ = seeded_graph(rmat_scale=10, edge_factor=8, grid_side=1024, seed=5)
+    k = 120000
+    base = n0 + 3 * np.arange(k, dtype=np.int32)
+    ts = np.concatenate([base, base + 1, base + 2]); td = np.concatenate([base + 1, base + 2, base])
+    n = n0 + 3 * k
+    s = np.concatenate([s, ts]).astype(np.int32); d = np.concatenate([d, td]).astype(np.int32)
+    csr = O.build_csr(n, s, d)
+    exp = O.tarjan_canonical(csr[0], csr[1])
+    g = Graph.from_edges(n, s, d)
+    st = State(g)
+    r = st.run(2)
+    assert n - r["trimmed_first"] - r["first_scc_size"] - r["trimmed_second"] >= 1 << 20   # live at the split
+    assert r["num_wcc_classes"] > k
+    assert np.array_equal(st.canonical_labels(), exp)
+    st.free(); g.free()
+
+
 def test_long_path_all_trimmed(gpu):
     n = 300000
     s = np.arange(n - 1); _check(n, s, s + 1)
