@@ -174,7 +174,8 @@ int scc_impl_wcc(const scc_graph* g, scc_state* s) {
 
 // ------------------------------------------------------------------ weak-component split
 // Union-find over the live same-colour edges: every live vertex ends with
-// uf[v] = smallest vertex of its weakly connected component inside its colour.
+// uf[v] = the root of its weakly connected component inside its colour (the
+// member of largest uf_rank).
 // Components are unions of SCCs, so they are valid independent classes, and
 // hooking converges in a few passes whatever the diameter (min-reach label
 // propagation above needs O(diameter) passes on grids and long cycles).
@@ -189,14 +190,24 @@ __device__ __forceinline__ int32_t uf_find(int32_t* __restrict__ uf, int32_t x) 
     return x;
 }
 
+// Roots are linked in the order of a bijective hash of their ids, not of the
+// ids themselves: on a row-major grid, lowest-id linking chains parents along
+// the rows and every find walks those chains.  Any total order keeps the
+// concurrent linking acyclic, and the final root of a component is its
+// vertex of largest hash whatever order the unions run in.
+__device__ __forceinline__ uint32_t uf_rank(int32_t x) {
+    uint32_t h = (uint32_t)x * 0x9E3779B1u;
+    return h ^ (h >> 16);
+}
+
 __device__ __forceinline__ void uf_union(int32_t* __restrict__ uf, int32_t a, int32_t b) {
     for (;;) {
         a = uf_find(uf, a);
         b = uf_find(uf, b);
         if (a == b) return;
-        int32_t hi = max(a, b), lo = min(a, b);
-        if (atomicCAS(uf + hi, hi, lo) == hi) return;
-        a = hi; b = lo;
+        int32_t lo = uf_rank(a) < uf_rank(b) ? a : b, hi = lo == a ? b : a;
+        if (atomicCAS(uf + lo, lo, hi) == lo) return;
+        a = lo; b = hi;
     }
 }
 
