@@ -305,9 +305,10 @@ struct LocalPush {
     int32_t* buf;          // warp's shared list: items
     int32_t* bb;           //   and their adjacency range [bb, be) in the item's direction
     int32_t* be;
-    int32_t* x0;           //   and, for an item of at most three neighbours, those
+    int32_t* x0;           //   and, for an item of at most four neighbours, those
     int32_t* x1;           //   neighbours (x0 = PRE_NONE when not preloaded)
     int32_t* x2;
+    int32_t* x3;
     int32_t count;         // warp-uniform
     int32_t pushed;        // items added since the last work-counter update
     int32_t* q; int32_t* tail; int32_t* work; int64_t qcap; int32_t* err;
@@ -332,12 +333,12 @@ struct LocalPush {
         __syncwarp();
     }
     // Items spilled to the global queue lose their range (the taker reloads it).
-    __device__ __forceinline__ void operator()(bool p, int32_t item, int32_t b, int32_t e, int32_t n0, int32_t n1, int32_t n2) {
+    __device__ __forceinline__ void operator()(bool p, int32_t item, int32_t b, int32_t e, int32_t n0, int32_t n1, int32_t n2, int32_t n3) {
         int lane = threadIdx.x & 31;
         unsigned bal = __ballot_sync(0xFFFFFFFFu, p);
         if (p) {
             int32_t pos = count + __popc(bal & ((1u << lane) - 1u));
-            buf[pos] = item; bb[pos] = b; be[pos] = e; x0[pos] = n0; x1[pos] = n1; x2[pos] = n2;
+            buf[pos] = item; bb[pos] = b; be[pos] = e; x0[pos] = n0; x1[pos] = n1; x2[pos] = n2; x3[pos] = n3;
         }
         int32_t k = __popc(bal);
         count += k;
@@ -351,7 +352,7 @@ struct LocalPush {
 // a claim loads the claimed vertex's range in the same round trip as the
 // atomic, so the next hop starts at the adjacency read.
 __device__ __forceinline__ void expand_warp_async(const RoundArgs& a, bool valid, int32_t it, int32_t b, int32_t e,
-                                                  int32_t x0, int32_t x1, int32_t x2, LocalPush& push,
+                                                  int32_t x0, int32_t x1, int32_t x2, int32_t x3, LocalPush& push,
                                                   long long* edge_acc) {
     int lane = threadIdx.x & 31;
     int32_t dir = 0, c = 0;
@@ -383,7 +384,7 @@ __device__ __forceinline__ void expand_warp_async(const RoundArgs& a, bool valid
                 p = visit(a, w, lc, ld);
                 if (p) { wb = __ldg(off + w); we = __ldg(off + w + 1); }
             }
-            push(p, w | (ld << DIR_SHIFT), wb, we, PRE_NONE, 0, 0);
+            push(p, w | (ld << DIR_SHIFT), wb, we, PRE_NONE, 0, 0, 0);
         }
     }
     int32_t mydeg = deg <= 32 ? deg : 0;
@@ -391,14 +392,14 @@ __device__ __forceinline__ void expand_warp_async(const RoundArgs& a, bool valid
     const int32_t* adj = dir ? a.r_node_idx : a.node_idx;
     const int32_t* off = dir ? a.r_begin : a.begin;
     const unsigned bit = 1u << dir;
-    const bool pre = x0 != PRE_NONE;   // at most three neighbours, already loaded
+    const bool pre = x0 != PRE_NONE;   // at most four neighbours, already loaded
     for (int32_t j0 = 0; j0 < maxd; j0 += 4) {
         int32_t w[4], wb[4], we[4];
         bool p[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             p[u] = (j0 + u) < mydeg;
-            w[u] = p[u] ? (pre ? (u == 0 ? x0 : u == 1 ? x1 : x2) : __ldg(adj + b + j0 + u)) : 0;
+            w[u] = p[u] ? (pre ? (u == 0 ? x0 : u == 1 ? x1 : u == 2 ? x2 : x3) : __ldg(adj + b + j0 + u)) : 0;
         }
         // the neighbour's range is loaded with its mark and colour (speculatively:
         // most neighbours on a narrow frontier are new), so the claim that
@@ -418,22 +419,23 @@ __device__ __forceinline__ void expand_warp_async(const RoundArgs& a, bool valid
             p[u] = p[u] && !(mk[u] & bit) && col[u] == c;
             old[u] = p[u] ? atomicOr(reinterpret_cast<unsigned*>(a.mark + (w[u] & ~3)), bit << ((w[u] & 3) * 8u)) : 0u;
         }
-        // a claimed vertex of at most three neighbours brings them along, loaded
+        // a claimed vertex of at most four neighbours brings them along, loaded
         // while its claim is in flight: its own expansion then starts at the
         // neighbours' marks instead of an adjacency read
-        int32_t n0[4], n1[4], n2[4];
+        int32_t n0[4], n1[4], n2[4], n3[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             int32_t dg = we[u] - wb[u];
-            bool small = p[u] && dg <= 3;
+            bool small = p[u] && dg <= 4;
             n0[u] = small ? (dg >= 1 ? __ldg(adj + wb[u]) : -1) : PRE_NONE;
             n1[u] = small && dg >= 2 ? __ldg(adj + wb[u] + 1) : -1;
             n2[u] = small && dg >= 3 ? __ldg(adj + wb[u] + 2) : -1;
+            n3[u] = small && dg >= 4 ? __ldg(adj + wb[u] + 3) : -1;
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) p[u] = p[u] && ((old[u] >> ((w[u] & 3) * 8u)) & bit) == 0u;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) push(p[u], w[u] | (dir << DIR_SHIFT), wb[u], we[u], n0[u], n1[u], n2[u]);
+        for (int u = 0; u < 4; ++u) push(p[u], w[u] | (dir << DIR_SHIFT), wb[u], we[u], n0[u], n1[u], n2[u], n3[u]);
     }
 }
 
@@ -446,13 +448,14 @@ __global__ void __launch_bounds__(ASYNC_THREADS, 1) k_reach_async(RoundArgs a, i
     __shared__ int32_t sx0[ASYNC_THREADS / 32][WBUF];
     __shared__ int32_t sx1[ASYNC_THREADS / 32][WBUF];
     __shared__ int32_t sx2[ASYNC_THREADS / 32][WBUF];
+    __shared__ int32_t sx3[ASYNC_THREADS / 32][WBUF];
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int32_t* head = a.ctr + CTR_AHEAD;
     int32_t* tail = a.ctr + CTR_ATAIL;
     int32_t* work = a.ctr + CTR_AWORK;
     int32_t* err = a.ctr + CTR_ERROR;
     int32_t* bail = a.ctr + CTR_ABAIL;
-    LocalPush push{sbuf[wid], sbeg[wid], send[wid], sx0[wid], sx1[wid], sx2[wid], 0, 0, q, tail, work, qcap, err, a.async_keep};
+    LocalPush push{sbuf[wid], sbeg[wid], send[wid], sx0[wid], sx1[wid], sx2[wid], sx3[wid], 0, 0, q, tail, work, qcap, err, a.async_keep};
     int idle = 0;
     uint32_t iter = 0;
     int32_t last_work = -1;
@@ -517,9 +520,10 @@ __global__ void __launch_bounds__(ASYNC_THREADS, 1) k_reach_async(RoundArgs a, i
         int32_t ix0 = (lane < k) ? push.x0[top] : PRE_NONE;
         int32_t ix1 = (lane < k) ? push.x1[top] : 0;
         int32_t ix2 = (lane < k) ? push.x2[top] : 0;
+        int32_t ix3 = (lane < k) ? push.x3[top] : 0;
         __syncwarp();
         push.count -= k;
-        expand_warp_async(a, lane < k, it, ib, ie, ix0, ix1, ix2, push, &my_edges);
+        expand_warp_async(a, lane < k, it, ib, ie, ix0, ix1, ix2, ix3, push, &my_edges);
         my_items += k;
         // the net change (pushed - expanded) accumulates in push.pushed and is
         // published every 8th iteration, before a spill makes items visible,
