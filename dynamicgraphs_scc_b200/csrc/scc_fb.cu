@@ -266,12 +266,18 @@ int scc_impl_resolve_all(const scc_graph* g, scc_state* s, bool classes_split) {
     double t_round = scc_trace_on() ? trace_ms() : 0.0;
     for (int round = 0; round < (1 << 30); ++round) {
         int32_t t = 0;
-        SCC_TRY(scc_impl_trim1(g, s, true, &t));
-        SCC_TRY(scc_impl_compact_live(g, s, false));
-        if (s->live_count == 0) break;
         int32_t classes = 0;
-        if (round == 0 && classes_split && t == 0) classes = -1;   // nothing changed since the caller's split
-        else SCC_TRY(scc_impl_uf_split(g, s, &classes));
+        if (round == 0 && classes_split) {
+            // the caller peeled to the fixpoint, compacted, then split: a split
+            // only recolours weakly disconnected parts, so no live vertex loses
+            // a same-colour neighbour and this round's peel would find nothing
+            classes = -1;
+        } else {
+            SCC_TRY(scc_impl_trim1(g, s, true, &t));
+            SCC_TRY(scc_impl_compact_live(g, s, false));
+            if (s->live_count == 0) break;
+            SCC_TRY(scc_impl_uf_split(g, s, &classes));
+        }
         int32_t live_before = s->live_count;
         int32_t found = 0, act = 0;
         SCC_TRY(scc_impl_fb_round(g, s, INT32_MIN, -1, &found, &act, true));
