@@ -136,8 +136,9 @@ static double now_ms() {
 }
 
 static int64_t graph_bytes(int32_t n, int64_t m) { return 8LL * ((int64_t)n + 1) + 8LL * m; }
-// state: per-vertex arrays, queues and per-colour slots (scc_state_create)
-static int64_t state_bytes(int32_t n) { return 140LL * (int64_t)n + 4096; }
+// state: per-vertex arrays, queues and per-colour slots (scc_state_create),
+// plus the 8-byte counts within colours a later peel allocates at first use
+static int64_t state_bytes(int32_t n) { return 148LL * (int64_t)n + 4096; }
 // an update: new CSR + transpose, deleted flags, sorted keys, temporaries
 static int64_t update_bytes(int32_t n, int64_t m, int64_t k_ins, int64_t k_del) {
     return 10LL * (m + k_ins) + 64LL * (k_ins + k_del) + 16LL * (int64_t)n + (1 << 20);
