@@ -505,7 +505,6 @@ static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     s->cnt_valid = !s->prefinished;      // the residue of finished vertices is not a count
     s->fresh = false;
     s->prefinished = false;
-    s->prefinished = false;
     return SCC_OK;
 }
 
@@ -706,9 +705,9 @@ __global__ void k_trim1_overflow_edges(TrimArgs a, const int32_t* __restrict__ i
     block_count_add(a.ctr + CTR_COUNT, cnt);
 }
 
-// The colour a trimmed vertex had is needed to re-check its neighbours; it is
-// recovered from any live neighbour?  No: the overflow list stores vertices
-// already set to -2, so their old colour is saved alongside by this kernel.
+// Re-checking an overflowed vertex's neighbours needs the colour it had before
+// it was trimmed (the list holds vertices already set to -2): this kernel
+// copies it from the snapshot, alongside the list.
 __global__ void k_save_colors(const int32_t* __restrict__ items, int32_t n, const int32_t* __restrict__ saved_src,
                               int32_t* __restrict__ out) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
