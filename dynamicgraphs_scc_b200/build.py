@@ -26,6 +26,7 @@ CU_SOURCES = [
     "scc_trim.cu",
     "scc_fb.cu",
     "scc_reach.cu",
+    "scc_tile.cu",
     "scc_wcc.cu",
     "scc_run.cu",
     "scc_gen.cu",

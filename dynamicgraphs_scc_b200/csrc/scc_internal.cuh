@@ -25,6 +25,10 @@ int scc_cuda_status(cudaError_t e, const char* what, const char* file, int line)
 
 // ---------------------------------------------------------------- constants
 #define SCC_THREADS 256
+// Host loops that repeat a device pass until a counter reads zero (peel
+// overflow rounds, level releases) shrink their list every round, so they end
+// well before this; reaching it reports SCC_ERR_TIMEOUT instead of a partial result.
+#define SCC_HOST_ROUND_LIMIT 1000000
 #define SCC_WCC_HIGH_DEG_FLAG 0x20000000   // scc_weak.cc:141-146
 #define SCC_WCC_ROOT_MASK 0x1FFFFFFF
 #define SCC_WCC_HIGH_DEG 50                // scc_weak.cc:143
@@ -104,6 +108,9 @@ struct scc_state {
     long long* hoff = nullptr;       // [2n+64] prefix of their degrees
     uint8_t* mark = nullptr;         // [n rounded to 4] reachability marks (bit0 FW, bit1 BW)
     int32_t* aux = nullptr;          // [n] per-vertex scratch (trim2 mates, pivot slots...)
+    int32_t* tq = nullptr;           // tile drain inboxes [tq_cap], kept at -1 between uses (allocated at first use)
+    int64_t tq_cap = 0;
+    int32_t* tctr = nullptr;         // tile drain counters (allocated at first use)
     int32_t* block_sums = nullptr;   // scan scratch
     int32_t* ctr = nullptr;          // device counters [CTR_MAX]
     int32_t* h_ctr = nullptr;        // pinned host mirror [CTR_MAX]
@@ -141,7 +148,7 @@ struct scc_state {
 
     // defaults from a B200 sweep on the mixed R-MAT + grid workload (fewer
     // resident warps in the drain mean less contention on its queue)
-    scc_tuning tune = {14, 24, 1 << 14, 1, 16, 1, 4096};
+    scc_tuning tune = {14, 24, 1 << 14, 1, 16, 1, 4096, 1 << 20, 2048};
 
     // kernel ledger (scc_state_profile): device time and algorithmic bytes of
     // the asynchronous reachability drain, timed with events on `stream`

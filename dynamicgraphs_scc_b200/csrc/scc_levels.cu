@@ -230,7 +230,8 @@ static int levels_on_device(const scc_graph* g, cudaStream_t st, int32_t* d_leve
     // Rounds: overflowed releases expanded by a list launch, hubs edge-parallel
     // (their releases join the overflow list).  Each node is released once,
     // so the lists together hold at most n and the rounds end.
-    for (int round = 0; round < 1000000; ++round) {
+    for (int round = 0;; ++round) {
+        SCC_REQUIRE(round < SCC_HOST_ROUND_LIMIT, SCC_ERR_TIMEOUT, "topological levels: no fixpoint after %d rounds", round);
         int32_t c[4] = {0, 0, 0, 0};
         SCC_CUDA(cudaMemcpyAsync(c, ctr.p, sizeof(c), cudaMemcpyDeviceToHost, st));
         SCC_CUDA(cudaStreamSynchronize(st));

@@ -10,7 +10,6 @@
 // overflow lists, the overflowed vertices' colours and the counters) lives in
 // the file-scope array below, which every GPU that loads this library holds
 // until the process exits.
-#include <mutex>
 #include "scc_internal.cuh"
 
 // Scratch layout (int32 words): snapshot | overflow A | overflow B | item colours | counters.
@@ -22,21 +21,18 @@ int scc_trim1_with_scratch(int32_t n, const int32_t* begin, const int32_t* node_
                            int32_t* ovf_a, int32_t* ovf_b, int32_t* item_colors, int32_t* ctr, cudaStream_t st,
                            int32_t* trimmed);
 
-// Device address of the scratch array, looked up once per device with that
-// device current.  In host code the array's name is only a host-side stand-in.
-static std::mutex g_setup_mutex;
-static int32_t* g_scratch_addr[64] = {nullptr};
-
-static int scratch_for_device(int device, int32_t** out) {
-    SCC_REQUIRE(device >= 0 && device < 64, SCC_ERR_INVALID, "device %d out of range", device);
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_trim1_scratch);
-        if (e != cudaSuccess) return scc_cuda_status(e, "cudaGetSymbolAddress(g_trim1_scratch)", __FILE__, __LINE__);
-        g_scratch_addr[device] = (int32_t*)p;
-    }
-    *out = g_scratch_addr[device];
+// Device address of the scratch array on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// with the device current.  The lookup is cheap and runs on every call, so an
+// address never outlives the context it came from (a cudaDeviceReset between
+// calls makes the next call look it up afresh).  With lazy module loading the
+// first lookup on a device is what loads this library's module there and
+// reserves the array.
+static int scratch_for_current_device(int32_t** out) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_trim1_scratch);
+    if (e != cudaSuccess) return scc_cuda_status(e, "cudaGetSymbolAddress(g_trim1_scratch)", __FILE__, __LINE__);
+    *out = (int32_t*)p;
     return SCC_OK;
 }
 
@@ -51,11 +47,11 @@ extern "C" int scc_trim1_noalloc(int32_t n, const int32_t* d_begin, const int32_
     SCC_REQUIRE(n == 0 || (d_begin && d_node_idx && d_r_begin && d_r_node_idx && d_color && d_scc), SCC_ERR_INVALID,
                 "NULL device array");
     *trimmed = 0;
-    if (n == 0) return SCC_OK;
-    int device = 0;
-    SCC_CUDA(cudaGetDevice(&device));
+    // the scratch is reserved on this device before anything else, so a call
+    // with n = 0 at start-up makes every later call allocation-free
     int32_t* base = nullptr;
-    SCC_TRY(scratch_for_device(device, &base));
+    SCC_TRY(scratch_for_current_device(&base));
+    if (n == 0) return SCC_OK;
     const int64_t M = SCC_NOALLOC_MAX_NODES;
     return scc_trim1_with_scratch(n, d_begin, d_node_idx, d_r_begin, d_r_node_idx, d_color, d_scc, base, base + M,
                                   base + 2 * M, base + 3 * M, base + 4 * M, (cudaStream_t)stream, trimmed);

@@ -26,6 +26,7 @@
 #include <stdlib.h>
 #include <algorithm>
 #include "scc_round.cuh"
+#include "scc_tile.cuh"
 
 // switch points come from the state's tunables (scc_tuning)
 #define ASYNC_EMPTY (-1)
@@ -590,6 +591,24 @@ static double now_ms() {
     return t.tv_sec * 1e3 + t.tv_nsec * 1e-6;
 }
 
+// The tile drain takes a round's narrow frontiers when the round has enough
+// live vertices and its live id range splits into tiles that fit shared
+// memory.  The live list is ascending, so its ends give the range.
+static bool tile_round(scc_state* s, int32_t* lo, int32_t* hi) {
+    if (s->tune.tile_min_live <= 0 || s->live_count < s->tune.tile_min_live) return false;
+    if (*lo < 0) {
+        int32_t ends[2] = {0, 0};
+        if (cudaMemcpyAsync(ends, s->live, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+            cudaMemcpyAsync(ends + 1, s->live + s->live_count - 1, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            s->stream) != cudaSuccess ||
+            cudaStreamSynchronize(s->stream) != cudaSuccess)
+            return false;
+        *lo = ends[0];
+        *hi = ends[1];
+    }
+    return scc_impl_tile_eligible(s, *lo, *hi);
+}
+
 // Direction choice (Beamer's rule as in the reference's BFS state machine,
 // gm_bfs_template.h:418-487): go bottom-up when the next frontier's edges
 // times bu_alpha exceed the edges of the vertices being traversed; stay
@@ -610,6 +629,7 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
                      ? s->tune.async_after : 0;
     bool bottom_up = false;
     double t0 = scc_trace_on() ? now_ms() : 0.0;
+    int32_t live_lo = -1, live_hi = -1;     // live id range, read once when the tile drain is considered
     while (qlen > 0) {
         const char* mode;
         bool synced = false;      // the counters on the host already hold this step's results
@@ -619,6 +639,17 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
             SCC_LAUNCHED(s);
             narrow = 0;
             mode = "bottom-up";
+        } else if (qlen <= s->tune.async_max && narrow >= s->tune.async_after && tile_round(s, &live_lo, &live_hi)) {
+            // narrow frontier over a large live range: the tile drain
+            int32_t handed = 0;
+            SCC_TRY(scc_impl_reach_tile(g, s, a, qin, qlen, qout, live_lo, live_hi, &handed));
+            if (handed == 0) return SCC_OK;
+            qlen = handed;
+            int32_t* t = qin; qin = qout; qout = t;
+            narrow = 0;
+            bottom_up = false;
+            if (scc_trace_on()) fprintf(stderr, "[scc] reach tile handed back %d items\n", qlen);
+            continue;
         } else if (qlen <= s->tune.async_max && narrow >= s->tune.async_after) {
             int64_t qcap = 2LL * s->n + 64;
             SCC_CUDA(cudaMemcpyAsync(s->aq, qin, sizeof(int32_t) * (size_t)qlen, cudaMemcpyDeviceToDevice, s->stream));

@@ -223,6 +223,7 @@ extern "C" int scc_state_free(scc_state* s) {
     cudaSetDevice(s->device);
     cudaFree(s->color); cudaFree(s->scc); cudaFree(s->wcc); cudaFree(s->live); cudaFree(s->live_tmp);
     cudaFree(s->qa); cudaFree(s->qb); cudaFree(s->aq); cudaFree(s->uf); cudaFree(s->hq); cudaFree(s->hoff); cudaFree(s->cnt); cudaFree(s->ccnt); cudaFree(s->mark); cudaFree(s->aux); cudaFree(s->block_sums);
+    cudaFree(s->tq); cudaFree(s->tctr);
     cudaFree(s->ctr);
     if (s->h_ctr) cudaFreeHost(s->h_ctr);
     cudaFree(s->slot_key); cudaFree(s->slot_pivot); cudaFree(s->slot_fw); cudaFree(s->slot_bw); cudaFree(s->slot_count);
@@ -299,6 +300,8 @@ extern "C" int scc_state_set_tuning(scc_state* s, const scc_tuning* t) {
     if (t->async_keep > 0) s->tune.async_keep = t->async_keep;
     if (t->async_blocks_per_sm > 0) s->tune.async_blocks_per_sm = t->async_blocks_per_sm;
     if (t->huge_deg > 0) s->tune.huge_deg = t->huge_deg;
+    if (t->tile_min_live != 0) s->tune.tile_min_live = t->tile_min_live > 0 ? t->tile_min_live : -1;
+    if (t->tile_min_span > 0) s->tune.tile_min_span = t->tile_min_span;
     return SCC_OK;
 }
 

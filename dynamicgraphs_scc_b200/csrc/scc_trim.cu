@@ -477,7 +477,8 @@ static int trim1_counting(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     // Rounds: overflowed trims are expanded by a list launch, hubs edge-parallel
     // (their trims join the overflow list).  Every vertex is trimmed once, so
     // the lists together never exceed n and the rounds end.
-    for (int round = 0; round < 1000000; ++round) {
+    for (int round = 0;; ++round) {
+        SCC_REQUIRE(round < SCC_HOST_ROUND_LIMIT, SCC_ERR_TIMEOUT, "Trim1: no fixpoint after %d rounds", round);
         SCC_TRY(scc_sync_counters(s));
         total += s->h_ctr[CTR_COUNT];
         int32_t novf = s->h_ctr[CTR_OVERFLOW];
@@ -598,7 +599,8 @@ static int trim1_coloured(const scc_graph* g, scc_state* s, int32_t* trimmed) {
     if (nseeds > 0) {
         k_count_peel<true><<<scc_blocks(nseeds, SCC_THREADS, 148 * 8), SCC_THREADS, 0, s->stream>>>(a, nseeds, s->qb, 1);
         SCC_LAUNCHED(s);
-        for (int round = 0; round < 1000000; ++round) {
+        for (int round = 0;; ++round) {
+            SCC_REQUIRE(round < SCC_HOST_ROUND_LIMIT, SCC_ERR_TIMEOUT, "Trim1: no fixpoint after %d rounds", round);
             SCC_TRY(scc_sync_counters(s));
             total += s->h_ctr[CTR_COUNT];
             int32_t novf = s->h_ctr[CTR_OVERFLOW];
@@ -766,7 +768,8 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
     s->fresh = false;
     s->prefinished = false;
     int64_t total = 0;
-    for (int round = 0; round < 1000000; ++round) {
+    for (int round = 0;; ++round) {
+        SCC_REQUIRE(round < SCC_HOST_ROUND_LIMIT, SCC_ERR_TIMEOUT, "Trim1: no fixpoint after %d rounds", round);
         SCC_TRY(scc_sync_counters(s));
         total += s->h_ctr[CTR_COUNT];
         int32_t novf = s->h_ctr[CTR_OVERFLOW];
@@ -788,8 +791,11 @@ int scc_impl_trim1(const scc_graph* g, scc_state* s, bool use_live, int32_t* tri
 
 // Trim1 to the fixpoint over all n vertices of caller-owned arrays, with every
 // scratch buffer supplied by the caller (snapshot, two overflow lists and the
-// overflow items' colours: n ints each; ctr: CTR_MAX ints).  Same kernels and
-// sweep as scc_do_global_trim1; used by the allocation-free entry point.
+// overflow items' colours: n ints each; ctr: CTR_MAX ints).  It computes the
+// same fixpoint as scc_do_global_trim1 with the scanning peel over all
+// vertices (k_trim1_sweep, whose cascades overflow to a list expanded a warp
+// per item by k_trim1_overflow) rather than the counting peel, which needs the
+// state's per-vertex count words; used by the allocation-free entry point.
 int scc_trim1_with_scratch(int32_t n, const int32_t* begin, const int32_t* node_idx, const int32_t* r_begin,
                            const int32_t* r_node_idx, int32_t* color, int32_t* scc, int32_t* snapshot,
                            int32_t* ovf_a, int32_t* ovf_b, int32_t* item_colors, int32_t* ctr, cudaStream_t st,
@@ -807,7 +813,8 @@ int scc_trim1_with_scratch(int32_t n, const int32_t* begin, const int32_t* node_
     k_trim1_sweep<<<scc_blocks(n, SCC_THREADS, 148 * 8), SCC_THREADS, 0, st>>>(a, nullptr, n);
     SCC_CUDA(cudaPeekAtLastError());
     int64_t total = 0;
-    for (int round = 0; round < 1000000; ++round) {
+    for (int round = 0;; ++round) {
+        SCC_REQUIRE(round < SCC_HOST_ROUND_LIMIT, SCC_ERR_TIMEOUT, "Trim1: no fixpoint after %d rounds", round);
         SCC_CUDA(cudaMemcpyAsync(h_ctr, ctr, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
         SCC_CUDA(cudaStreamSynchronize(st));
         total += h_ctr[CTR_COUNT];

@@ -250,7 +250,7 @@ class State:
 
     def set_tuning(self, **kw) -> None:
         """Change traversal tunables (keys of scc_tuning); unspecified keys keep their value."""
-        t = capi.Tuning(*([0] * 7))
+        t = capi.Tuning(*([0] * len(capi.Tuning._fields_)))
         for k, v in kw.items():
             if not hasattr(t, k):
                 raise KeyError(k)

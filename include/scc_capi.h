@@ -173,8 +173,14 @@ typedef struct scc_tuning {
     int32_t async_keep;           /* items a warp keeps for itself before sharing (16, max 192) */
     int32_t async_blocks_per_sm;  /* resident blocks per SM in the drain (1, max 8) */
     int32_t huge_deg;             /* degree above which a top-down item is expanded edge-parallel (4096) */
+    int32_t tile_min_live;        /* rounds with at least this many live vertices drain narrow frontiers
+                                     tile by tile (one id range per SM, marks in shared memory) (1 << 20);
+                                     negative = never */
+    int32_t tile_min_span;        /* smallest id range of a tile (2048) */
 } scc_tuning;
 int scc_state_get_tuning(scc_state* s, scc_tuning* t);
+/* Fields <= 0 keep their current value, except tile_min_live, where a negative
+ * value turns the tile drain off. */
 int scc_state_set_tuning(scc_state* s, const scc_tuning* t);
 /* Autotuner: times up to max_trials full decompositions (method) of g under
  * candidate tunings, keeps the fastest in s, resets s, and reports it. */
@@ -215,13 +221,18 @@ int scc_create_trim1_compact(const scc_graph* g, scc_state* s, int32_t* live_cou
  * colour) on caller-owned device arrays of the current device: the CSR and
  * transpose (n+1 / m ints), d_color and d_scc (n ints, updated in place).
  * The scratch lives in one file-scope __device__ array of
- * 4 * SCC_NOALLOC_MAX_NODES + 128 ints (about 16 MiB) that every GPU loading
- * the library holds until exit; n above SCC_NOALLOC_MAX_NODES is rejected with
- * SCC_ERR_INVALID.  The first call on a device looks up that array's device
- * address (make that first call before any stream capture).  All calls share
- * the array, so calls that overlap on the GPU (other streams, other host
- * threads) race; serialise them.  Work is ordered on `stream` (cudaStream_t as
- * void*, NULL = legacy default stream) and the call returns once it is done. */
+ * 4 * SCC_NOALLOC_MAX_NODES + 128 ints (about 16 MiB); n above
+ * SCC_NOALLOC_MAX_NODES is rejected with SCC_ERR_INVALID.  With CUDA's lazy
+ * module loading (the default) the array is reserved on a device when the
+ * first call on that device looks up its address, so call once with n = 0
+ * (NULL arrays are accepted then) at start-up, before any stream capture: that
+ * call reserves the array and does nothing else, and from then on the device
+ * holds it until the process exits.  Every call looks the address up again,
+ * with no allocation.  All calls share the array, so calls that overlap on the
+ * GPU (other streams, other host threads) race; serialise them.  Work is
+ * ordered on `stream` (cudaStream_t as void*, NULL = legacy default stream);
+ * the call reads its counters back on that stream and returns once the work
+ * is done. */
 #define SCC_NOALLOC_MAX_NODES (1 << 20)
 int scc_trim1_noalloc(int32_t n, const int32_t* d_begin, const int32_t* d_node_idx,
                       const int32_t* d_r_begin, const int32_t* d_r_node_idx,

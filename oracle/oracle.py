@@ -88,6 +88,9 @@ def ref():
         L.ref_method2.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P, C.c_int, C.c_int, _I32P,
                                   C.POINTER(C.c_double)]
         L.ref_method2.restype = C.c_int
+        L.ref_method.argtypes = [C.c_int, C.c_int32, C.c_int64, _I32P, _I32P, C.c_int, C.c_int, _I32P,
+                                 C.POINTER(C.c_double)]
+        L.ref_method.restype = C.c_int
         L.ref_tarjan.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P, _I32P, C.POINTER(C.c_double)]
         L.ref_tarjan.restype = C.c_int
         L.ref_method7_levels.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P, C.c_int64, _I32P, _I32P, _I32P,
@@ -191,8 +194,8 @@ class _QuietStdout:
         return False
 
 
-def ref_method2(csr, threads=None, pin=False, quiet=True):
-    """The reference's own method-2 pipeline: (canonical labels, run ms)."""
+def ref_method(method, csr, threads=None, pin=False, quiet=True):
+    """The reference's own method-0/1/2 pipeline (my_main::run): (canonical labels, run ms)."""
     b, a = csr[0], csr[1]
     n = b.size - 1
     out = np.empty(max(n, 1), np.int32)
@@ -200,12 +203,17 @@ def ref_method2(csr, threads=None, pin=False, quiet=True):
     th = threads or os.cpu_count() or 1
     if quiet:
         with _QuietStdout():
-            rc = ref().ref_method2(n, a.size, _p(b), _p(a), th, int(pin), _p(out), C.byref(ms))
+            rc = ref().ref_method(method, n, a.size, _p(b), _p(a), th, int(pin), _p(out), C.byref(ms))
     else:
-        rc = ref().ref_method2(n, a.size, _p(b), _p(a), th, int(pin), _p(out), C.byref(ms))
+        rc = ref().ref_method(method, n, a.size, _p(b), _p(a), th, int(pin), _p(out), C.byref(ms))
     if rc != 0:
-        raise RuntimeError("reference method 2 failed")
+        raise RuntimeError(f"reference method {method} failed")
     return canonical(out[:n]), ms.value
+
+
+def ref_method2(csr, threads=None, pin=False, quiet=True):
+    """The reference's own method-2 pipeline: (canonical labels, run ms)."""
+    return ref_method(2, csr, threads=threads, pin=pin, quiet=quiet)
 
 
 def ref_tarjan(csr):

@@ -42,14 +42,17 @@ static double now_ms() {
     return t.tv_sec * 1000.0 + t.tv_usec * 0.001;
 }
 
-extern "C" int ref_method2(int32_t n, int64_t m, const int32_t* begin, const int32_t* node_idx, int threads,
-                           int pin, int32_t* scc_out, double* ms_out) {
+// Method 0, 1 or 2 of my_main::run (src/scc_main.cc:120-145) with its own
+// phase selection, timed over run() like the reference's timer.
+extern "C" int ref_method(int method, int32_t n, int64_t m, const int32_t* begin, const int32_t* node_idx,
+                          int threads, int pin, int32_t* scc_out, double* ms_out) {
+    if (method < 0 || method > 2) return 2;
     gm_rt_set_num_threads(threads);
     my_main T;
-    char a0[] = "2";
+    char a0[2] = {(char)('0' + method), 0};
     char* av[] = {a0};
     if (!T.check_args(1, av)) return 1;
-    met_algo = 2;
+    met_algo = method;
     build_graph(T.G, n, m, begin, node_idx);
     if (pin) T.pin_CPU();
     T.prepare();
@@ -65,7 +68,13 @@ extern "C" int ref_method2(int32_t n, int64_t m, const int32_t* begin, const int
     finalize_analyze();
     delete[] G_SCC;
     G_SCC = NULL;
+    met_algo = 2;
     return 0;
+}
+
+extern "C" int ref_method2(int32_t n, int64_t m, const int32_t* begin, const int32_t* node_idx, int threads,
+                           int pin, int32_t* scc_out, double* ms_out) {
+    return ref_method(2, n, m, begin, node_idx, threads, pin, scc_out, ms_out);
 }
 
 struct tarjan_job {
