@@ -147,31 +147,58 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(sm)}
 
 
-def run_reference(args, workload):
-    """Reference arm: the reference's own OpenMP method-2 pipeline on the host cores."""
+def host_csr(kw):
+    """Seeded edge list of a workload -> forward CSR on the host (self-loops and
+    duplicates removed; the oracle's dedup leaves the edges sorted by (source,
+    target), so the CSR is its offsets and targets).  Input preparation for the
+    reference's own engine, which builds its reverse edges itself."""
     from oracle import oracle as O
     from dynamicgraphs_scc_b200 import generate_edges_host
-    kw = CPU_SAMPLES[workload]
     n, s, d = generate_edges_host(**kw)
     s, d = O.dedup_edges(s, d, n=n)
-    csr = O.build_csr(n, s, d)
+    b = np.zeros(n + 1, np.int32)
+    np.cumsum(np.bincount(s, minlength=n), out=b[1:])
+    return n, b, np.ascontiguousarray(d, np.int32)
+
+
+# The reference's method per workload.  Method 2 (do_baseline_global_wcc_fb)
+# keeps a pool of 65,536 node sets, one per weak component, and takes from it
+# with no bound check (init_node_set_pool(65536) in src/scc_weak.cc:35,
+# get_node_set_from_pool :24-29): the 4096 x 4096 oriented grid leaves more
+# weak components than that after trimming, and method 2 reads past the pool
+# and crashes.  On graphs holding that grid the reference arm runs method 1
+# (do_baseline_global_fb: Trim1 + global FW-BW + Trim1 + FW-BW), the
+# reference's method that completes there.
+REF_METHOD = {"c2": 1, "grid4096": 1}
+REF_METHOD_NOTE = ("method 2 overruns its 65,536-entry node-set pool (src/scc_weak.cc:24-35) on this graph's "
+                   "oriented grid and crashes; method 1 is the reference's method that completes on it")
+
+
+def run_reference(args, workload, full=True):
+    """Reference arm: the reference's own OpenMP pipeline on the host cores, on
+    the full workload (full=True) or on the 1/16 sample of CPU_SAMPLES."""
+    from oracle import oracle as O
+    kw = WORKLOADS[workload] if full else CPU_SAMPLES[workload]
+    n, b, a = host_csr(kw)
     threads = os.cpu_count() or 1
+    method = REF_METHOD.get(workload, 2) if full else 2
     kind = "reference" if O.ref_available() else "port"
     times = []
     for i in range(args.warmup + args.steps):
         if kind == "reference":
-            _, ms = O.ref_method2(csr, threads=threads)
+            _, ms = O.ref_method(method, (b, a), threads=threads)
         else:
             t0 = time.perf_counter()
-            O.tarjan_canonical(csr[0], csr[1])
+            O.tarjan_canonical(b, a)
             ms = (time.perf_counter() - t0) * 1e3
         if i >= args.warmup:
             times.append(ms)
     ms = statistics.mean(times)
-    gteps = s.size / (ms * 1e-3) / 1e9
-    sample = f"{WORKLOAD_NAMES[workload]} scaled to " + json.dumps(kw) + f": n={n} m={s.size}"
+    gteps = a.size / (ms * 1e-3) / 1e9
+    what = "full configuration" if full else "1/16 sample, " + json.dumps(kw)
+    sample = f"{WORKLOAD_NAMES[workload]} ({what}): n={n} m={a.size}, method {method}"
     return gteps, ms, dict(value=gteps, unit="GTEPS", cores=threads if kind == "reference" else 1, kind=kind,
-                           sample=sample, ms=ms)
+                           sample=sample, ms=ms, method=method, n=n, m=int(a.size))
 
 
 def train_pivot_model(device):
@@ -260,15 +287,38 @@ def bench_batched(args, local_rank):
 SERVE = dict(rmat_scale=22, edge_factor=16, seed=2022)
 
 
-def bench_serving(args, local_rank):
+def _tarjan_equal(b, a, labels):
+    """Oracle check of one serving snapshot (runs in a spawned worker process)."""
+    from oracle import oracle as O
+    return bool(np.array_equal(O.tarjan_canonical(b, a), labels))
+
+
+def _pct(xs, p):
+    return xs[min(len(xs) - 1, int(p * (len(xs) - 1) + 0.5))] if xs else None
+
+
+def bench_serving(args, local_rank, batches_n=None, sustain_n=None):
     """Streaming updates against a device-resident R-MAT s22 ef16 graph through the
     serving loop: batches arrive Poisson (mean 2 ms), sizes log-uniform in
     [1e3, 1e6] edges, 70% inserts / 30% deletes of existing edges, endpoints
     degree-proportional (ends of random existing edges); every 100 batches the
-    labels are checked against a full Tarjan recomputation of the current graph."""
+    labels are checked against a full Tarjan recomputation of the current graph
+    (the checks run in a pool of host processes while serving goes on).
+
+    Two phases.  "configured": the arrival process as configured, which offers
+    more than one session's in-order updates can serve, with backpressure (a
+    backlog limit in edges, and an age limit) so the queue stays bounded;
+    offered, served and shed load are reported.  "sustainable": the same batch
+    distribution at a mean gap the service sustains (1.25 x the configured
+    phase's mean service time per admitted batch), where p50/p99 describe the
+    system rather than the length of the run.  Returns the JSON line."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
     import torch
-    from oracle import oracle as O
     from dynamicgraphs_scc_b200 import Graph, Server
+    batches_n = args.batches if batches_n is None else batches_n
+    sustain_n = args.sustain_batches if sustain_n is None else sustain_n
+    pool = ProcessPoolExecutor(max_workers=min(8, os.cpu_count() or 1), mp_context=mp.get_context("spawn"))
     torch.cuda.set_device(local_rank)
     g = Graph.generate(**SERVE, device=local_rank)
     n, m0 = g.num_nodes(), g.num_edges()
@@ -277,57 +327,173 @@ def bench_serving(args, local_rank):
     sv = Server(num_slots=4, hbm_budget_bytes=96 << 30, device=local_rank)
     if args.coalesce > 1:
         sv.set_coalesce(args.coalesce)
+    sv.set_admission(args.admit_edges, args.admit_ms)
     sid = sv.add_graph(g)
     rng = np.random.default_rng(2022)
     lo, hi = np.log(1e3), np.log(1e6)
-    batches = []
-    for _ in range(args.batches):
+
+    def make_batch():
         k = int(np.exp(lo + rng.random() * (hi - lo)))
         ki = int(round(0.7 * k)); kd = k - ki
         ii = rng.integers(0, base_src.size, (2, ki))
         dd = rng.integers(0, base_src.size, kd)
-        batches.append((base_src[ii[0]], base_dst[ii[1]], base_src[dd], base_dst[dd]))
-    gaps = rng.exponential(2.0, args.batches)
-    checks, check_ok = 0, True
-    results = []
-    t0 = time.perf_counter()
-    due = 0.0
-    pending = []
-    for i, bt in enumerate(batches):
-        due += gaps[i] * 1e-3
-        delay = t0 + due - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        pending.append(sv.submit(sid, *bt))
-        if (i + 1) % 100 == 0 or i + 1 == len(batches):
-            results += [sv.wait(r) for r in pending]
-            pending = []
-            if (i + 1) % 100 == 0:
+        return base_src[ii[0]], base_dst[ii[1]], base_src[dd], base_dst[dd]
+
+    checks = []
+    counter = {"batches": 0}
+
+    def run_phase(count, mean_gap_ms):
+        results, shed, pending, offered = [], 0, [], 0
+        t_last = time.perf_counter()
+        gaps = rng.exponential(mean_gap_ms, count)
+        t0 = time.perf_counter()
+        due = 0.0
+        for i in range(count):
+            bt = make_batch()
+            due += gaps[i] * 1e-3
+            delay = t0 + due - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            rid = sv.submit(sid, *bt)
+            edges = sum(x.size for x in bt)
+            offered += edges
+            if rid < 0:
+                shed += 1
+            else:
+                pending.append((rid, edges))
+            counter["batches"] += 1
+            t_last = time.perf_counter()
+            if counter["batches"] % 100 == 0:
+                results += [(sv.wait(r), e) for r, e in pending]
+                pending = []
                 cb, ca, _, _ = sv.session_csr(sid)
-                exp = O.tarjan_canonical(cb, ca)
-                checks += 1
-                check_ok = check_ok and bool(np.array_equal(sv.labels(sid), exp))
-    wall = time.perf_counter() - t0
+                checks.append(pool.submit(_tarjan_equal, cb, ca, sv.labels(sid)))
+        arrival_s = max(t_last - t0, 1e-9)
+        results += [(sv.wait(r), e) for r, e in pending]
+        wall = time.perf_counter() - t0
+        ok = [(r, e) for r, e in results if r["status"] == 0]
+        lat = sorted(r["latency_ms"] for r, _ in ok)
+        svc = sorted(r["ms_total"] for r, _ in ok)
+        served_edges = sum(e for _, e in ok)
+        return {"batches": count, "mean_gap_ms": round(mean_gap_ms, 3), "admitted": len(results),
+                "applied": len(ok), "shed_at_submit": shed,
+                "expired_in_queue": sum(r["status"] == 9 for r, _ in results),
+                "offered_updates_per_s": round(offered / arrival_s, 1),
+                "served_updates_per_s": round(served_edges / wall, 1),
+                "latency_ms": {"p50": round(_pct(lat, 0.5), 3) if lat else None,
+                               "p99": round(_pct(lat, 0.99), 3) if lat else None,
+                               "max": round(lat[-1], 3) if lat else None},
+                "service_ms": {"p50": round(_pct(svc, 0.5), 3) if svc else None,
+                               "p99": round(_pct(svc, 0.99), 3) if svc else None,
+                               "mean": round(float(np.mean(svc)), 3) if svc else None},
+                "wall_s": round(wall, 2)}
+
+    t_all = time.perf_counter()
+    configured = run_phase(batches_n, 2.0)
+    gap = 1.25 * (configured["service_ms"]["mean"] or 2.0)
+    sustainable = run_phase(sustain_n, gap) if sustain_n > 0 else None
+    sv.drain()
     st = sv.stats()
-    service = sorted(r["ms_total"] for r in results if r["status"] == 0)
-    pct = lambda xs, p: xs[min(len(xs) - 1, int(p * (len(xs) - 1) + 0.5))] if xs else None  # noqa: E731
     cb, _, _, _ = sv.session_csr(sid)
+    check_ok = [f.result() for f in checks]
+    pool.shutdown()
+    sv.free()
+    lat_ref = sustainable or configured
     line = {
         "metric": "streaming SCC updates: p50/p99 batch latency (ms) and updates/s",
-        "value": round(st["updates_per_s"], 1), "unit": "updates/s", "n_gpus": 1, "steps": len(results),
+        "value": configured["served_updates_per_s"], "unit": "updates/s", "n_gpus": 1,
+        "steps": configured["applied"] + (sustainable["applied"] if sustainable else 0),
         "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded)",
         "config": {"workload": "R-MAT s22 ef16 base, Poisson(2 ms) arrivals, batch log-uniform [1e3, 1e6], "
                                "70% insert / 30% delete, degree-proportional endpoints",
-                   "batches": len(results), "n": n, "m_before": m0, "m_after": int(cb[-1]), "slots": 4,
-                   "coalesce": args.coalesce, "device_updates": st["groups"]},
-        "latency_ms": {"p50": round(st["p50_ms"], 3), "p99": round(st["p99_ms"], 3), "max": round(st["max_ms"], 3)},
-        "service_ms": {"p50": round(pct(service, 0.5), 3), "p99": round(pct(service, 0.99), 3)},
-        "tarjan_checks": {"count": checks, "all_equal": check_ok},
-        "rejected": st["rejected"], "wall_s": round(wall, 2),
+                   "n": n, "m_before": m0, "m_after": int(cb[-1]), "slots": 4, "coalesce": args.coalesce,
+                   "admission": {"max_queued_edges": args.admit_edges, "max_queue_ms": args.admit_ms},
+                   "device_updates": st["groups"]},
+        "configured": configured,
+        "sustainable": sustainable,
+        "latency_ms": lat_ref["latency_ms"],
+        "tarjan_checks": {"count": len(check_ok), "all_equal": all(check_ok), "every": 100},
+        "wall_s": round(time.perf_counter() - t_all, 2),
     }
-    sv.free()
-    print(json.dumps(line))
+    return line
+
+
+def time_steps(st, stream, steps, warmup, mode=0):
+    """W untimed decompositions, then K timed ones (CUDA events on the state's stream)."""
+    import torch
+    for _ in range(warmup):
+        st.reset(); st.run(2, mode)
+    st.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True); ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    last = None
+    for _ in range(steps):
+        st.reset()
+        last = st.run(2, mode)
+    ev1.record(stream)
+    st.synchronize()
+    return ev0.elapsed_time(ev1) / steps, last
+
+
+def extra_rmat24(local_rank, steps=10, warmup=3):
+    """R-MAT s24 ef16 alone: the configuration whose whole-step roofline target is 40 %."""
+    import torch
+    from dynamicgraphs_scc_b200 import Graph, State
+    g = Graph.generate(**WORKLOADS["rmat24"], device=local_rank)
+    n, m = g.num_nodes(), g.num_edges()
+    st = State(g)
+    stream = torch.cuda.ExternalStream(st.stream(), device=local_rank)
+    ms, last = time_steps(st, stream, steps, warmup)
+    peak, kind = measured_peak_gbs()
+    ach = (16 * m + 20 * n + 8) / (ms * 1e-3) / 1e9
+    st.free(); g.free()
+    return {"workload": WORKLOAD_NAMES["rmat24"], "n": n, "m": m, "steps": steps, "warmup": warmup,
+            "ms_per_step": round(ms, 4), "value": round(m / (ms * 1e-3) / 1e9, 3), "unit": "GTEPS",
+            "roofline_step": {"bound": "hbm", "achieved": round(ach, 2), "peak": peak, "peak_kind": kind,
+                              "unit": "GB/s", "frac": round(ach / peak, 4)}}
+
+
+def extra_c3(local_rank, steps=5, warmup=3):
+    """Learned vs plain pivot on the planted-cycles configuration, and on the
+    mixed configuration (C2), each with labels compared."""
+    import torch
+    from dynamicgraphs_scc_b200 import Graph, State
+    model, info = train_pivot_model(local_rank)
+    out = {"pivot_model": info}
+    for name in ("c3", "c2"):
+        g = Graph.generate(**WORKLOADS[name], device=local_rank)
+        m = g.num_edges()
+        st = State(g)
+        st.set_pivot_model(model)
+        stream = torch.cuda.ExternalStream(st.stream(), device=local_rank)
+        p_ms, _ = time_steps(st, stream, steps, warmup, 0)
+        p_lab = st.canonical_labels()
+        l_ms, _ = time_steps(st, stream, steps, warmup, 1)
+        eq = bool(np.array_equal(p_lab, st.canonical_labels()))
+        st.free(); g.free()
+        out[name] = {"plain_ms": round(p_ms, 4), "learned_ms": round(l_ms, 4),
+                     "learned_speedup": round(p_ms / l_ms, 4), "labels_equal": eq,
+                     "plain_gteps": round(m / (p_ms * 1e-3) / 1e9, 3),
+                     "learned_gteps": round(m / (l_ms * 1e-3) / 1e9, 3)}
+    return out
+
+
+def default_extras(args, local_rank):
+    """Secondary configurations measured in the default run, so that its JSON
+    line carries all of the benchmark metric: R-MAT s24's roofline fraction,
+    learned vs plain pivot, and the streaming loop's p50/p99."""
+    out = {}
+    for name, fn in (("rmat24", lambda: extra_rmat24(local_rank)), ("learned_pivot", lambda: extra_c3(local_rank)),
+                     ("streaming", lambda: bench_serving(args, local_rank, batches_n=args.extra_batches,
+                                                         sustain_n=args.extra_batches // 4))):
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as exc:     # reported, never hidden
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"}
+        out[name + "_s"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 LEVELS = dict(rmat_scale=24, edge_factor=16, grid_side=4096, seed=2024)          # C2's graph
@@ -463,10 +629,20 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5", "levels"])
     ap.add_argument("--tune-trials", type=int, default=8)
-    ap.add_argument("--batches", type=int, default=200)
+    ap.add_argument("--batches", type=int, default=10000, help="c5: batches at the configured arrival rate")
+    ap.add_argument("--sustain-batches", type=int, default=2000,
+                    help="c5: batches at a rate the service sustains (0 = skip)")
+    ap.add_argument("--admit-edges", type=int, default=4000000,
+                    help="c5: backlog limit in queued edges (0 = none)")
+    ap.add_argument("--admit-ms", type=float, default=2000.0, help="c5: age limit of a queued batch (0 = none)")
     ap.add_argument("--coalesce", type=int, default=1, help="c5: queued batches of a session composed per update")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the secondary configurations of the default run (R-MAT s24, learned pivot, streaming)")
+    ap.add_argument("--extra-batches", type=int, default=1000, help="streaming batches measured in the default run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-sample", action="store_true",
+                    help="reference arm: time the 1/16 sample instead of the full configuration")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -480,7 +656,7 @@ def main():
                                   "update file per process, methods 5-11)"}))
             return
         if rank == 0:
-            bench_serving(args, local_rank)
+            print(json.dumps(bench_serving(args, local_rank)))
         return
 
     if args.workload == "levels":
@@ -508,15 +684,19 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        gteps, ms, cpu = run_reference(args, args.workload)
+        gteps, ms, cpu = run_reference(args, args.workload, full=not args.ref_sample)
         line = {"metric": "SCC GTEPS (edges / end-to-end decomposition time)", "value": round(gteps, 6),
                 "unit": "GTEPS", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded)",
-                "config": {"workload": WORKLOAD_NAMES[args.workload], "sample": cpu["sample"],
-                           "method": 2, "parallelism": f"replicas x{args.gpus}"},
+                "config": {"workload": WORKLOAD_NAMES[args.workload], "params": WORKLOADS[args.workload],
+                           "n": cpu["n"], "m": cpu["m"], "method": cpu["method"],
+                           "parallelism": f"host cores x{cpu['cores']} (rank 0 only)"},
+                "same_config": not args.ref_sample,
                 "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": round(gteps, 6), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if cpu["method"] != 2:
+            line["method_note"] = REF_METHOD_NOTE
         print(json.dumps(line))
         return
 
@@ -698,10 +878,15 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            _, _, cpu = run_reference(argparse.Namespace(steps=1, warmup=0), args.workload)
+            _, _, cpu = run_reference(argparse.Namespace(steps=1, warmup=0), args.workload, full=False)
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as exc:  # the baseline is reported, not required
             cpu = {"value": None, "unit": "GTEPS", "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
+
+    extras = None
+    if rank == 0 and world == 1 and args.workload == "c2" and not args.no_extras:
+        st.free(); g.free()                 # the headline graph is done with
+        extras = default_extras(args, local_rank)
 
     if dist is not None:
         dist.barrier()
@@ -733,6 +918,8 @@ def main():
         "stats": {k: last[k] for k in ("num_sccs", "first_scc_size", "trimmed_first", "trimmed_second",
                                         "num_wcc_classes", "traversal_steps")},
     }
+    if extras is not None:
+        line["extras"] = extras
     if learned:
         line["metric"] = "SCC GTEPS, learned pivot (plain pivot beside it)"
         line["plain_pivot"] = plain

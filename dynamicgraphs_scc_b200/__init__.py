@@ -8,7 +8,7 @@ kernels behind a C ABI (include/scc_capi.h).
 from .capi import SccError, lib  # noqa: F401
 from .engine import (  # noqa: F401
     METHOD_BASELINE, METHOD_GLOBAL_FB, METHOD_GLOBAL_WCC_FB, PIVOT_DEGREE, PIVOT_LEARNED,
-    Graph, PivotModel, Server, State, collect_pivot_records, condensation_graph, decompose_csr, device_count, gen_params, generate_batch_edges_host, generate_edges_host,
+    BatchPlan, Graph, PivotModel, Server, State, batch_autotune, collect_pivot_records, condensation_graph, decompose_csr, device_count, gen_params, generate_batch_edges_host, generate_edges_host,
     read_edge_list, read_scc_list, topological_levels, affected_levels,
 )
 

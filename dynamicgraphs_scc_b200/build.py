@@ -27,6 +27,7 @@ CU_SOURCES = [
     "scc_fb.cu",
     "scc_reach.cu",
     "scc_tile.cu",
+    "scc_batch.cu",
     "scc_wcc.cu",
     "scc_run.cu",
     "scc_gen.cu",

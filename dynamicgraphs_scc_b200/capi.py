@@ -16,8 +16,9 @@ LIB_PATH = os.path.join(_HERE, "lib", "libscc_b200.so")
 SCC_OK = 0
 STATUS_NAMES = {
     0: "SCC_OK", 1: "SCC_ERR_INVALID", 2: "SCC_ERR_CUDA", 3: "SCC_ERR_OOM", 4: "SCC_ERR_TIMEOUT",
-    5: "SCC_ERR_STATE", 6: "SCC_ERR_IO", 7: "SCC_ERR_NOT_FOUND", 8: "SCC_ERR_UNSUPPORTED",
+    5: "SCC_ERR_STATE", 6: "SCC_ERR_IO", 7: "SCC_ERR_NOT_FOUND", 8: "SCC_ERR_UNSUPPORTED", 9: "SCC_ERR_BUSY",
 }
+SCC_ERR_BUSY = 9
 SCC_BUILD_KEEP_ALL = 0
 SCC_BUILD_DEDUP = 1
 SCC_BUILD_NO_SELF_LOOPS = 2
@@ -65,7 +66,8 @@ class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_int64), ("rejected", C.c_int64), ("updates", C.c_int64),
                 ("max_inflight", C.c_int64), ("bytes_in_use", C.c_int64), ("p50_ms", C.c_double),
                 ("p99_ms", C.c_double), ("max_ms", C.c_double), ("updates_per_s", C.c_double),
-                ("groups", C.c_int64)]
+                ("groups", C.c_int64), ("offered_edges", C.c_int64), ("shed", C.c_int64), ("shed_edges", C.c_int64),
+                ("expired", C.c_int64), ("max_queued_edges", C.c_int64), ("offered_per_s", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -74,6 +76,21 @@ class ServerStats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [(k, C.c_int32) for k in ("bu_alpha", "bu_div", "async_max", "async_after", "async_keep",
                                          "async_blocks_per_sm", "huge_deg", "tile_min_live", "tile_min_span")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("blocks_per_sm", C.c_int32), ("warp_deg", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("graphs", C.c_int32), ("rounds", C.c_int32), ("levels", C.c_int32),
+                ("max_rounds", C.c_int32), ("host_submissions", C.c_int32), ("kernels", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -172,6 +189,11 @@ _SIGS = {
     "scc_read_edge_list": [C.c_char_p, C.c_int64, _I32P, _I32P, C.POINTER(C.c_int64), _I32P],
     "scc_affected_levels": [_P, _I32P, C.c_int32, C.c_int32, _I32P, C.c_int64, _I32P, _I32P, _I32P, _I32P],
     "scc_state_finish_unaffected": [_P, _I32P, _I32P, C.c_int32, _I32P],
+    "scc_batch_default_tuning": [C.POINTER(BatchTuning)],
+    "scc_batch_plan_create": [_P, _P, _I32P, C.c_int32, C.POINTER(BatchTuning), C.POINTER(_P)],
+    "scc_batch_plan_run": [_P, C.POINTER(BatchStats)],
+    "scc_batch_plan_free": [_P],
+    "scc_batch_autotune": [_P, _P, _I32P, C.c_int32, C.POINTER(BatchTuning), C.POINTER(C.c_double)],
     "scc_server_create": [C.c_int, C.c_int, C.c_int64, C.POINTER(_P)],
     "scc_server_add_graph": [_P, _P, _I32P],
     "scc_server_submit": [_P, C.c_int32, C.c_int64, _I32P, _I32P, C.c_int64, _I32P, _I32P, _I64P],
@@ -180,6 +202,7 @@ _SIGS = {
     "scc_release_cached_memory": [C.c_int],
     "scc_debug_inject": [C.c_int, C.c_int64],
     "scc_server_wait": [_P, C.c_int64, C.POINTER(RequestResult)],
+    "scc_server_set_admission": [_P, C.c_int64, C.c_double],
     "scc_server_drain": [_P],
     "scc_server_get_stats": [_P, C.POINTER(ServerStats)],
     "scc_server_labels": [_P, C.c_int32, _I32P],

@@ -49,6 +49,7 @@ extern "C" const char* scc_status_string(int status) {
         case SCC_ERR_IO: return "file error";
         case SCC_ERR_NOT_FOUND: return "not found";
         case SCC_ERR_UNSUPPORTED: return "unsupported";
+        case SCC_ERR_BUSY: return "busy (admission limit)";
         default: return "unknown status";
     }
 }

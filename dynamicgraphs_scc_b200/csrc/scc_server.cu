@@ -12,6 +12,13 @@
 // never fit the budget is rejected with SCC_ERR_OOM.  Latency = completion -
 // submission (host clock); p50/p99 and updates/s are kept.
 //
+// Backpressure (scc_server_set_admission, off by default): a submission that
+// would take the backlog of queued edges above a limit is refused with
+// SCC_ERR_BUSY, and a request that has waited longer than an age limit is
+// dropped (status SCC_ERR_BUSY) when a slot reaches it, so under overload the
+// queue and the latency of admitted requests stay bounded instead of growing
+// for the whole run.  Offered, served, shed and expired counts are kept.
+//
 // Coalescing (scc_server_set_coalesce, off by default): when a session's turn
 // comes with several of its requests queued, up to max_requests of them
 // (max_edges edges in all) are composed into one batch and applied by one
@@ -67,6 +74,11 @@ struct scc_server {
     int32_t coalesce = 1;        // requests per group (1 = off)
     int64_t coalesce_edges = 0;  // edge cap of a group
     double t_first = -1.0, t_last = 0.0;
+    int64_t max_queued = 0;      // admission: backlog limit in edges (0 = none)
+    double max_age_ms = 0.0;     //            age limit of a queued request (0 = none)
+    int64_t queued_edges = 0, max_queued_seen = 0;
+    int64_t offered_edges = 0, shed = 0, shed_edges = 0, expired = 0;
+    double t_last_submit = 0.0;
 };
 
 // ------------------------------------------------------------------ composition of queued batches
@@ -161,6 +173,19 @@ static void worker_main(scc_server* sv) {
                     ServerRequest* c = sv->reqs[*it].get();
                     ServerSession& s = sv->sessions[(size_t)c->session];
                     if (blocked[(size_t)c->session] || s.busy) { blocked[(size_t)c->session] = 1; continue; }
+                    if (sv->max_age_ms > 0 && now_ms() - c->t_submit > sv->max_age_ms) {
+                        // waited past the age limit: dropped, the session unchanged
+                        c->rc = SCC_ERR_BUSY;
+                        c->done = true;
+                        c->t_done = now_ms();
+                        sv->expired++;
+                        sv->completed++;
+                        sv->queued_edges -= (int64_t)(c->ins_src.size() + c->del_src.size());
+                        sv->queue.erase(it);
+                        sv->cv_done.notify_all();
+                        rejected_one = true;
+                        break;
+                    }
                     if (sv->in_use + c->est_bytes > sv->budget) {
                         if (sv->inflight == 0) {   // can never fit: reject
                             c->rc = SCC_ERR_OOM;
@@ -168,6 +193,7 @@ static void worker_main(scc_server* sv) {
                             c->t_done = now_ms();
                             sv->rejected++;
                             sv->completed++;
+                            sv->queued_edges -= (int64_t)(c->ins_src.size() + c->del_src.size());
                             sv->queue.erase(it);
                             sv->cv_done.notify_all();
                             rejected_one = true;
@@ -178,6 +204,7 @@ static void worker_main(scc_server* sv) {
                     }
                     r = c;
                     ses = &s;
+                    sv->queued_edges -= (int64_t)(c->ins_src.size() + c->del_src.size());
                     sv->queue.erase(it);
                     break;
                 }
@@ -196,6 +223,8 @@ static void worker_main(scc_server* sv) {
                     int64_t ni = n_ins + (int64_t)c->ins_src.size(), nd = n_del + (int64_t)c->del_src.size();
                     int64_t bytes = update_bytes(ses->g->n, ses->g->m, ni, nd);
                     if (ni + nd > sv->coalesce_edges || sv->in_use + bytes > sv->budget) break;
+                    if (sv->max_age_ms > 0 && now_ms() - c->t_submit > sv->max_age_ms) break;
+                    sv->queued_edges -= (int64_t)(c->ins_src.size() + c->del_src.size());
                     grp.push_back(c);
                     n_ins = ni; n_del = nd; grp_bytes = bytes;
                     it = sv->queue.erase(it);
@@ -258,6 +287,14 @@ extern "C" int scc_server_set_coalesce(scc_server* sv, int32_t max_requests, int
     return SCC_OK;
 }
 
+extern "C" int scc_server_set_admission(scc_server* sv, int64_t max_queued_edges, double max_queue_ms) {
+    SCC_REQUIRE(sv && max_queued_edges >= 0 && max_queue_ms >= 0, SCC_ERR_INVALID, "bad argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->max_queued = max_queued_edges;
+    sv->max_age_ms = max_queue_ms;
+    return SCC_OK;
+}
+
 extern "C" int scc_server_create(int device, int num_slots, int64_t hbm_budget_bytes, scc_server** out) {
     SCC_REQUIRE(out && num_slots >= 1 && num_slots <= 64 && hbm_budget_bytes > 0, SCC_ERR_INVALID, "bad argument");
     SCC_CUDA(cudaSetDevice(device));
@@ -302,17 +339,34 @@ extern "C" int scc_server_submit(scc_server* sv, int32_t session, int64_t n_ins,
     SCC_REQUIRE(sv && request_id, SCC_ERR_INVALID, "NULL argument");
     SCC_REQUIRE(n_ins >= 0 && n_del >= 0 && (n_ins == 0 || (ins_src && ins_dst)) && (n_del == 0 || (del_src && del_dst)),
                 SCC_ERR_INVALID, "bad batch");
+    *request_id = -1;
+    {
+        // backpressure before the copy: a refused batch costs nothing
+        std::lock_guard<std::mutex> lk(sv->mu);
+        SCC_REQUIRE(session >= 0 && session < (int32_t)sv->sessions.size(), SCC_ERR_INVALID, "no session %d", session);
+        double t = now_ms();
+        if (sv->t_first < 0) sv->t_first = t;
+        sv->t_last_submit = t;
+        sv->offered_edges += n_ins + n_del;
+        if (sv->max_queued > 0 && sv->queued_edges + n_ins + n_del > sv->max_queued) {
+            sv->shed++;
+            sv->shed_edges += n_ins + n_del;
+            scc_set_error("serving queue holds %lld edges; limit %lld", (long long)sv->queued_edges,
+                          (long long)sv->max_queued);
+            return SCC_ERR_BUSY;
+        }
+    }
     auto r = std::make_unique<ServerRequest>();
     r->ins_src.assign(ins_src, ins_src + n_ins); r->ins_dst.assign(ins_dst, ins_dst + n_ins);
     r->del_src.assign(del_src, del_src + n_del); r->del_dst.assign(del_dst, del_dst + n_del);
     std::lock_guard<std::mutex> lk(sv->mu);
-    SCC_REQUIRE(session >= 0 && session < (int32_t)sv->sessions.size(), SCC_ERR_INVALID, "no session %d", session);
     const ServerSession& s = sv->sessions[(size_t)session];
     r->session = session;
     r->id = sv->next_id++;
     r->est_bytes = update_bytes(s.g->n, s.g->m, n_ins, n_del);
     r->t_submit = now_ms();
-    if (sv->t_first < 0) sv->t_first = r->t_submit;
+    sv->queued_edges += n_ins + n_del;
+    sv->max_queued_seen = std::max(sv->max_queued_seen, sv->queued_edges);
     *request_id = r->id;
     sv->queue.push_back(r->id);
     sv->reqs[r->id] = std::move(r);
@@ -362,6 +416,13 @@ extern "C" int scc_server_get_stats(scc_server* sv, scc_server_stats* out) {
     out->max_inflight = sv->max_inflight;
     out->bytes_in_use = sv->in_use;
     out->groups = sv->groups;
+    out->offered_edges = sv->offered_edges;
+    out->shed = sv->shed;
+    out->shed_edges = sv->shed_edges;
+    out->expired = sv->expired;
+    out->max_queued_edges = sv->max_queued_seen;
+    double offer_span = sv->t_last_submit - sv->t_first;
+    out->offered_per_s = offer_span > 0 ? sv->offered_edges / (offer_span * 1e-3) : 0.0;
     return SCC_OK;
 }
 

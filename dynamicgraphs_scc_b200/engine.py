@@ -519,6 +519,51 @@ def collect_pivot_records(graph: Graph, capacity: int = 1 << 20, per_round: int 
         st.free()
 
 
+class BatchPlan:
+    """One persistent launch over a disjoint union of independent graphs (offsets
+    give each graph's vertex range), captured once into a CUDA graph; run()
+    replays it.  Results land in the state (canonical_labels etc.)."""
+
+    def __init__(self, graph: Graph, state: "State", offsets, tuning: dict | None = None):
+        self.graph, self.state = graph, state
+        self.offsets = np.ascontiguousarray(offsets, np.int32)
+        t = None
+        if tuning is not None:
+            t = capi.BatchTuning()
+            call("scc_batch_default_tuning", C.byref(t))
+            for k, v in tuning.items():
+                setattr(t, k, int(v))
+        h = C.c_void_p()
+        call("scc_batch_plan_create", graph.handle, state.handle, i32p(self.offsets), int(self.offsets.size - 1),
+             C.byref(t) if t is not None else None, C.byref(h))
+        self._h = h
+
+    def run(self) -> dict:
+        st = capi.BatchStats()
+        call("scc_batch_plan_run", self._h, C.byref(st))
+        return st.as_dict()
+
+    def free(self) -> None:
+        if self._h is not None:
+            call("scc_batch_plan_free", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def batch_autotune(graph: Graph, state: "State", offsets):
+    """Successive-halving search of the batched run's launch shape; (tuning dict, ms on the whole batch)."""
+    offs = np.ascontiguousarray(offsets, np.int32)
+    t = capi.BatchTuning()
+    ms = C.c_double()
+    call("scc_batch_autotune", graph.handle, state.handle, i32p(offs), int(offs.size - 1), C.byref(t), C.byref(ms))
+    return t.as_dict(), ms.value
+
+
 class Server:
     """Serving loop: device-resident graphs updated by streamed edge batches
     (continuous batching over worker slots, HBM-budget admission)."""
@@ -539,11 +584,22 @@ class Server:
         return sid.value
 
     def submit(self, session: int, ins_src=(), ins_dst=(), del_src=(), del_dst=()) -> int:
+        """Queues a batch; returns its request id, or -1 when backpressure refused it
+        (the queue is over its admission limit)."""
         a, b, c, d = _i32(ins_src), _i32(ins_dst), _i32(del_src), _i32(del_dst)
         rid = C.c_int64()
-        call("scc_server_submit", self._h, session, int(a.size), i32p(a), i32p(b), int(c.size), i32p(c), i32p(d),
-             C.byref(rid))
+        rc = capi.lib().scc_server_submit(self._h, session, int(a.size), i32p(a), i32p(b), int(c.size), i32p(c),
+                                          i32p(d), C.byref(rid))
+        if rc == capi.SCC_ERR_BUSY:
+            return -1
+        if rc != 0:
+            raise capi.SccError(rc, "scc_server_submit", capi.lib().scc_last_error().decode(errors="replace"))
         return rid.value
+
+    def set_admission(self, max_queued_edges: int = 0, max_queue_ms: float = 0.0) -> None:
+        """Backpressure: refuse submissions beyond a backlog of queued edges, drop
+        requests older than max_queue_ms when a slot reaches them (0 = no limit)."""
+        call("scc_server_set_admission", self._h, int(max_queued_edges), float(max_queue_ms))
 
     def wait(self, request_id: int) -> dict:
         r = capi.RequestResult()

@@ -45,6 +45,7 @@ extern "C" {
 #define SCC_ERR_IO           6   /* file could not be read or written */
 #define SCC_ERR_NOT_FOUND    7   /* no vertex of the requested colour (NIL_NODE in the reference) */
 #define SCC_ERR_UNSUPPORTED  8   /* method or flag not offered by this engine */
+#define SCC_ERR_BUSY         9   /* serving loop: the queue is over its admission limit; retry later */
 
 #define SCC_NIL_NODE (-1)        /* gm_graph::NIL_NODE */
 #define SCC_COLOR_INIT (-1)
@@ -377,11 +378,49 @@ int scc_affected_levels(const scc_graph* dag, const int32_t* levels, int32_t max
 int scc_state_finish_unaffected(scc_state* s, const int32_t* levels, const int32_t* affected, int32_t max_level,
                                 int32_t* finished);
 
+/* ---- batched small graphs (no counterpart in the reference, which decomposes one
+ * graph per process) -------------------------------------------------------------------- */
+/* Many independent graphs stored as one disjoint union (graph i owns the vertices
+ * [offsets[i], offsets[i+1]), no edge leaves a graph) are decomposed by ONE
+ * persistent launch: each block takes whole graphs, largest first, and runs the
+ * method (Trim1 to the fixpoint, then rounds of pivot / FW+BW / classify / peel over
+ * every class of the graph) inside the block.  The plan captures the run (counter
+ * reset, the launch, the counters back) into a CUDA graph once; each run is one
+ * graph launch.  Results land in the state's colour and SCC arrays, so
+ * scc_canonical_labels and the other output calls work on the union. */
+typedef struct scc_batch_tuning {
+    int32_t threads;              /* threads per block (512) */
+    int32_t blocks_per_sm;        /* resident blocks per SM (2) */
+    int32_t warp_deg;             /* lists longer than this are expanded by a whole warp (32) */
+} scc_batch_tuning;
+typedef struct scc_batch_stats {
+    double ms_total;              /* device time of the run (events around the graph launch) */
+    int32_t graphs, rounds, levels, max_rounds;
+    int32_t host_submissions;     /* graph launches of the run (1) */
+    int32_t kernels;              /* kernel launches inside it (1) */
+} scc_batch_stats;
+typedef struct scc_batch_plan scc_batch_plan;
+int scc_batch_default_tuning(scc_batch_tuning* t);
+/* offsets: host array of num_graphs + 1 vertex offsets, 0 .. g's vertex count.  The
+ * plan keeps g and s (both must outlive it); tuning may be NULL (defaults). */
+int scc_batch_plan_create(const scc_graph* g, scc_state* s, const int32_t* offsets, int32_t num_graphs,
+                          const scc_batch_tuning* tuning, scc_batch_plan** out);
+/* One run: every graph decomposed; synchronises.  stats may be NULL. */
+int scc_batch_plan_run(scc_batch_plan* p, scc_batch_stats* stats);
+int scc_batch_plan_free(scc_batch_plan* p);
+/* Autotuner of the batched run: successive halving over threads per block, blocks
+ * per SM and the warp cut-off.  Every candidate runs on a prefix of the graphs
+ * (a quarter, then half, then all of them), the faster half goes on; the winner
+ * is returned in *best with its time on the whole batch. */
+int scc_batch_autotune(const scc_graph* g, scc_state* s, const int32_t* offsets, int32_t num_graphs,
+                       scc_batch_tuning* best, double* best_ms);
+
 /* ---- serving loop (no counterpart in the reference, whose dynamic methods read one
  * update file per process, src/common_main.h:500-732) ----------------------------------- */
 typedef struct scc_server scc_server;
 typedef struct scc_request_result {
-    int status;                 /* SCC_OK, or SCC_ERR_OOM when the batch can never fit the budget */
+    int status;                 /* SCC_OK; SCC_ERR_OOM when the batch can never fit the budget;
+                                   SCC_ERR_BUSY when it waited longer than the admission age limit */
     int32_t session;
     double latency_ms;          /* completion - submission */
     double queue_ms;            /* admission - submission */
@@ -391,6 +430,12 @@ typedef struct scc_server_stats {
     int64_t completed, rejected, updates, max_inflight, bytes_in_use;
     double p50_ms, p99_ms, max_ms, updates_per_s;
     int64_t groups;             /* device updates applied (fewer than completed when requests coalesce) */
+    int64_t offered_edges;      /* edges of every submission, shed ones included */
+    int64_t shed;               /* submissions refused at the queue limit (SCC_ERR_BUSY from submit) */
+    int64_t shed_edges;
+    int64_t expired;            /* requests dropped at the age limit (status SCC_ERR_BUSY) */
+    int64_t max_queued_edges;   /* largest backlog seen (edges queued, not yet admitted) */
+    double offered_per_s;       /* offered edges / (last submission - first submission) */
 } scc_server_stats;
 
 /* num_slots worker threads; admission keeps resident graphs + admitted batches
@@ -408,6 +453,14 @@ int scc_server_submit(scc_server* sv, int32_t session, int64_t n_ins, const int3
  * unless a later request of the group deletes that pair) and applied by one
  * update.  Each request of a group then reports the group's result. */
 int scc_server_set_coalesce(scc_server* sv, int32_t max_requests, int64_t max_edges);
+/* Backpressure, off by default (0 = no limit).  A submission whose edges would
+ * take the backlog (edges queued and not yet admitted, all sessions) above
+ * max_queued_edges is refused: submit returns SCC_ERR_BUSY, queues nothing and
+ * sets *request_id to -1.  A request still queued max_queue_ms after its
+ * submission is dropped when a slot reaches it: it completes with status
+ * SCC_ERR_BUSY and changes nothing.  Either way the client decides whether to
+ * resend; the graph stays as the admitted requests left it. */
+int scc_server_set_admission(scc_server* sv, int64_t max_queued_edges, double max_queue_ms);
 int scc_server_wait(scc_server* sv, int64_t request_id, scc_request_result* out);
 int scc_server_drain(scc_server* sv);
 int scc_server_get_stats(scc_server* sv, scc_server_stats* out);

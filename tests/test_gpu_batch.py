@@ -58,3 +58,74 @@ def test_autotune_keeps_labels(gpu):
     st.run(2)
     csr = O.build_csr(n, s, d)
     assert np.array_equal(st.canonical_labels(), O.tarjan_canonical(csr[0], csr[1]))
+
+
+def test_persistent_batch_plan_equals_tarjan_twice(gpu):
+    """The one-launch batched run (each block decomposes whole graphs; the run
+    replayed from a captured CUDA graph) gives Tarjan's labels, twice in a row
+    on the same plan, with one host submission and one kernel per run."""
+    from dynamicgraphs_scc_b200 import BatchPlan
+    n, offs, s, d = host_batch()
+    csr = O.build_csr(n, s, d)
+    exp = O.tarjan_canonical(csr[0], csr[1])
+    g, goffs = Graph.generate_batch(**KW)
+    st = State(g)
+    plan = BatchPlan(g, st, goffs)
+    for _ in range(2):
+        r = plan.run()
+        assert r["host_submissions"] == 1 and r["kernels"] == 1 and r["graphs"] == len(goffs) - 1
+        assert np.array_equal(st.canonical_labels(), exp)
+    plan.free()
+
+
+@pytest.mark.parametrize("tuning", [dict(threads=256, blocks_per_sm=1, warp_deg=8),
+                                    dict(threads=1024, blocks_per_sm=2, warp_deg=64)])
+def test_batch_plan_tunings_and_structures(gpu, tuning):
+    """Launch shapes and warp cut-offs change speed only: graphs of long
+    cycles, long paths, a bidirectional star (one list far above the warp
+    cut-off) and 3-cycles, batched with random graphs, all equal Tarjan."""
+    from dynamicgraphs_scc_b200 import BatchPlan
+    parts, src, dst, offs = [], [], [], [0]
+    rng = np.random.default_rng(4)
+    specs = [("cycle", 5000), ("path", 4000), ("star", 3000), ("tri", 900), ("rand", 2000), ("rand", 64)]
+    for kind, k in specs:
+        base = offs[-1]
+        if kind == "cycle":
+            a = np.arange(k); b = (a + 1) % k
+        elif kind == "path":
+            a = np.arange(k - 1); b = a + 1
+        elif kind == "star":
+            leaves = np.arange(1, k)
+            a = np.concatenate([np.zeros(k - 1, int), leaves]); b = np.concatenate([leaves, np.zeros(k - 1, int)])
+        elif kind == "tri":
+            t = 3 * np.arange(k // 3)
+            a = np.concatenate([t, t + 1, t + 2]); b = np.concatenate([t + 1, t + 2, t])
+        else:
+            a, b = rng.integers(0, k, (2, 3 * k))
+        src.append(a + base); dst.append(b + base)
+        offs.append(base + k)
+    n = offs[-1]
+    s = np.concatenate(src).astype(np.int32); d = np.concatenate(dst).astype(np.int32)
+    csr = O.build_csr(n, s, d)
+    exp = O.tarjan_canonical(csr[0], csr[1])
+    g = Graph.from_edges(n, s, d)
+    st = State(g)
+    plan = BatchPlan(g, st, np.asarray(offs, np.int32), tuning=tuning)
+    plan.run()
+    assert np.array_equal(st.canonical_labels(), exp)
+    plan.free()
+
+
+def test_batch_autotune_successive_halving(gpu):
+    from dynamicgraphs_scc_b200 import BatchPlan, batch_autotune
+    n, offs, s, d = host_batch()
+    csr = O.build_csr(n, s, d)
+    exp = O.tarjan_canonical(csr[0], csr[1])
+    g, goffs = Graph.generate_batch(**KW)
+    st = State(g)
+    best, ms = batch_autotune(g, st, goffs)
+    assert ms > 0 and best["threads"] in (256, 512, 1024)
+    plan = BatchPlan(g, st, goffs, tuning=best)
+    plan.run()
+    assert np.array_equal(st.canonical_labels(), exp)
+    plan.free()

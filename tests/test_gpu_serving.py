@@ -140,3 +140,40 @@ def test_coalesced_requests_equal_sequential(gpu):
         ss, dd = apply_batch(ss, dd, *b)
     csr = O.build_csr(n, ss, dd)
     assert np.array_equal(l_co, O.tarjan_canonical(csr[0], csr[1]))
+
+
+def test_backpressure_sheds_and_expires(gpu):
+    """Admission by backlog and age: with one slot and a backlog limit of three
+    batches, a burst of twenty batches is partly refused at submit (request id
+    -1); with a short age limit, queued requests may also be dropped when a
+    slot reaches them (status SCC_ERR_BUSY).  Whatever was refused or dropped
+    changed nothing: the labels equal Tarjan of the graph with only the
+    applied batches, in order, and the counts add up."""
+    n, s, d, _ = seeded_graph(rmat_scale=12, edge_factor=6, seed=21)
+    rng = np.random.default_rng(8)
+    batches = []
+    for _ in range(20):
+        pick = rng.integers(0, len(s), 300)
+        batches.append((rng.integers(0, n, 700).astype(np.int32), rng.integers(0, n, 700).astype(np.int32),
+                        s[pick].astype(np.int32), d[pick].astype(np.int32)))
+    sv = Server(num_slots=1, hbm_budget_bytes=8 << 30)
+    sid = sv.add_graph(Graph.from_edges(n, s, d))
+    sv.set_admission(max_queued_edges=3000, max_queue_ms=2.0)
+    rids = [sv.submit(sid, *b) for b in batches]
+    res = [sv.wait(r) if r >= 0 else None for r in rids]
+    sv.drain()
+    lab = sv.labels(sid)
+    st = sv.stats()
+    sv.free()
+    shed = sum(r is None for r in res)
+    applied = [b for b, r in zip(batches, res) if r is not None and r["status"] == 0]
+    expired = sum(r is not None and r["status"] == 9 for r in res)
+    assert shed >= 1 and st["shed"] == shed and st["expired"] == expired
+    assert st["offered_edges"] == 20 * 1000 and st["shed_edges"] == 1000 * shed
+    assert st["completed"] == 20 - shed
+    assert len(applied) >= 1 and st["max_queued_edges"] <= 3000
+    ss, dd = s, d
+    for b in applied:
+        ss, dd = apply_batch(ss, dd, *b)
+    csr = O.build_csr(n, ss, dd)
+    assert np.array_equal(lab, O.tarjan_canonical(csr[0], csr[1]))
