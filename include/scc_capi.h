@@ -183,8 +183,10 @@ int scc_state_get_tuning(scc_state* s, scc_tuning* t);
 /* Fields <= 0 keep their current value, except tile_min_live, where a negative
  * value turns the tile drain off. */
 int scc_state_set_tuning(scc_state* s, const scc_tuning* t);
-/* Autotuner: times up to max_trials full decompositions (method) of g under
- * candidate tunings, keeps the fastest in s, resets s, and reports it. */
+/* Autotuner: successive halving over the tunables with a budget of max_trials full
+ * decompositions (method) of g: a seeded sample of settings (the current one among
+ * them) is timed once each, the faster half twice each, and so on; the winner is kept
+ * in s (which is reset) and reported with its mean time. */
 int scc_autotune(const scc_graph* g, scc_state* s, int method, int max_trials, scc_tuning* best, double* best_ms);
 
 /* ---- colour (src/scc_color.cc) --------------------------------------------------------- */
