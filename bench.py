@@ -201,6 +201,50 @@ def run_reference(args, workload, full=True):
                            sample=sample, ms=ms, method=method, n=n, m=int(a.size))
 
 
+def run_reference_cuda(args, workload):
+    """The reference's own CUDA engine (src_CUDA method 2, compiled for sm_100a)
+    on this GPU, on the full workload: a comparator, not the drop-in.  Its
+    labels are checked against the reference's own Tarjan digest where one is
+    recorded (its WCC stops after 100 propagation passes, scc_cuda_weak.cu:489,
+    and its host FW-BW takes at most 999,999 work items, scc_cuda_fb_seq2.cu,
+    so on long-diameter graphs it may not finish every vertex)."""
+    import hashlib
+    from oracle import oracle as O
+    from dynamicgraphs_scc_b200 import generate_edges_host
+    if not O.ref_cuda_available():
+        return {"impl": "reference-cuda", "unavailable": "the reference's CUDA engine was not built (oracle/Makefile)"}
+    kw = WORKLOADS[workload]
+    n, s, d = generate_edges_host(**kw)
+    s, d = O.dedup_edges(s, d, n=n)
+    csr = O.build_csr(n, s, d)
+    m = int(csr[1].size)
+    del s, d
+    threads = os.cpu_count() or 1
+    times, lab = [], None
+    for i in range(args.warmup + args.steps):
+        lab, ms = O.ref_cuda_method2(csr, threads=threads)
+        if i >= args.warmup:
+            times.append(ms)
+    ms = statistics.mean(times)
+    finished = int(np.count_nonzero(lab >= 0))
+    canon = O.canonical(np.where(lab >= 0, lab, np.arange(n, dtype=np.int32)).astype(np.int32))
+    digest = hashlib.sha256(np.ascontiguousarray(canon, dtype="<i4").tobytes()).hexdigest()
+    ref = {}
+    p = os.path.join(ROOT, "tests", "golden", "fullsize_digests.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            ref = json.load(f).get(workload, {})
+    return {"impl": "reference-cuda", "metric": "SCC GTEPS (edges / end-to-end decomposition time)",
+            "value": round(m / (ms * 1e-3) / 1e9, 6), "unit": "GTEPS", "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 3), "higher_is_better": True, "dtype": "int32", "n_gpus": 1,
+            "config": {"workload": WORKLOAD_NAMES[workload], "params": kw, "n": n, "m": m, "method": 2,
+                       "host_threads": threads,
+                       "timing": "host clock over the reference's own timed region (scc_cuda_main.cpp R1..R2)"},
+            "vertices_finished": finished,
+            "labels_equal_reference_tarjan": (digest == ref.get("labels_sha256")) if ref else None,
+            "num_sccs": int(np.count_nonzero(canon == np.arange(n, dtype=np.int32)))}
+
+
 def train_pivot_model(device):
     """The learned pivot proposer, trained as the configuration asks: records of
     plain runs on 64 seeded R-MAT graphs of scales 18-22 (ef16), then Adam on the
@@ -235,7 +279,7 @@ def bench_batched(args, local_rank):
     import torch
     from dynamicgraphs_scc_b200 import BatchPlan, Graph, State, batch_autotune
     torch.cuda.set_device(local_rank)
-    g, offs = Graph.generate_batch(**BATCH, device=local_rank)
+    g, offs = Graph.generate_batch(**{**BATCH, "num_graphs": args.batch_graphs}, device=local_rank)
     n, m = g.num_nodes(), g.num_edges()
     st = State(g)
     t0 = time.perf_counter()
@@ -279,7 +323,7 @@ def bench_batched(args, local_rank):
         "value": round(m / (ms * 1e-3) / 1e9, 4), "unit": "GTEPS", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded per graph)",
-        "config": {"workload": "4096 graphs, n log-uniform [1024, 65536], out-degree Poisson(6), 30% R-MAT / 70% "
+        "config": {"workload": f"{args.batch_graphs} graphs, n log-uniform [1024, 65536], out-degree Poisson(6), 30% R-MAT / 70% "
                                "uniform targets, self-loops and duplicates removed", "n": n, "m": m,
                    "autotuned": best, "autotune": {"method": "successive halving (1/8, 1/4, 1/2, all graphs)",
                                                    "seconds": round(tune_s, 2), "best_ms": round(tuned_ms, 3)},
@@ -638,9 +682,10 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5", "levels"])
     ap.add_argument("--tune-trials", type=int, default=8)
+    ap.add_argument("--batch-graphs", type=int, default=4096, help="c4: graphs in the batch")
     ap.add_argument("--batches", type=int, default=10000, help="c5: batches at the configured arrival rate")
     ap.add_argument("--sustain-batches", type=int, default=2000,
                     help="c5: batches at a rate the service sustains (0 = skip)")
@@ -691,6 +736,11 @@ def main():
             return
         if rank == 0:
             bench_batched(args, local_rank)
+        return
+
+    if args.impl == "reference-cuda":
+        if rank == 0:
+            print(json.dumps(run_reference_cuda(args, args.workload)))
         return
 
     if args.impl == "reference":

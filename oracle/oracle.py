@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libscc_ref.so")
 REF_CLI = os.path.join(HERE, "_ref", "scc")
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libscc_ref_cuda.so")
 
 _I32P = C.POINTER(C.c_int32)
 _U8P = C.POINTER(C.c_uint8)
@@ -214,6 +215,38 @@ def ref_method(method, csr, threads=None, pin=False, quiet=True):
 def ref_method2(csr, threads=None, pin=False, quiet=True):
     """The reference's own method-2 pipeline: (canonical labels, run ms)."""
     return ref_method(2, csr, threads=threads, pin=pin, quiet=quiet)
+
+
+_ref_cuda = None
+
+
+def ref_cuda_available() -> bool:
+    return os.path.exists(REF_CUDA_SO)
+
+
+def ref_cuda_method2(csr, threads=None, quiet=True):
+    """The reference's own CUDA method 2 (src_CUDA, built for sm_100a) on the
+    current GPU, from a CSR and its transpose: (canonical labels, run ms)."""
+    global _ref_cuda
+    if _ref_cuda is None:
+        L = C.CDLL(REF_CUDA_SO)
+        L.refcuda_method2.argtypes = [C.c_int32, C.c_int64, _I32P, _I32P, _I32P, _I32P, C.c_int, _I32P,
+                                      C.POINTER(C.c_double)]
+        L.refcuda_method2.restype = C.c_int
+        _ref_cuda = L
+    b, a, rb, ra = csr
+    n = b.size - 1
+    out = np.empty(max(n, 1), np.int32)
+    ms = C.c_double()
+    th = threads or os.cpu_count() or 1
+    if quiet:
+        with _QuietStdout():
+            rc = _ref_cuda.refcuda_method2(n, a.size, _p(b), _p(a), _p(rb), _p(ra), th, _p(out), C.byref(ms))
+    else:
+        rc = _ref_cuda.refcuda_method2(n, a.size, _p(b), _p(a), _p(rb), _p(ra), th, _p(out), C.byref(ms))
+    if rc != 0:
+        raise RuntimeError("reference CUDA method 2 failed")
+    return out[:n].copy(), ms.value
 
 
 def ref_tarjan(csr):
