@@ -527,11 +527,23 @@ def extra_c3(local_rank, steps=5, warmup=3):
         p_lab = st.canonical_labels()
         l_ms, _ = time_steps(st, stream, steps, warmup, 1)
         eq = bool(np.array_equal(p_lab, st.canonical_labels()))
+        # ceiling of any proposer that re-ranks the degree rule's equally good
+        # candidates: the same plain run under 15 other tie-breaks of the rule
+        salts = []
+        for salt in range(1, 16):
+            st.set_tuning(pivot_salt=salt)
+            ms_s, _ = time_steps(st, stream, 2, 1, 0)
+            salts.append(round(ms_s, 4))
+            eq = eq and bool(np.array_equal(p_lab, st.canonical_labels()))
+        st.set_tuning(pivot_salt=-1)                  # back to the default tie-break
         st.free(); g.free()
         out[name] = {"plain_ms": round(p_ms, 4), "learned_ms": round(l_ms, 4),
                      "learned_speedup": round(p_ms / l_ms, 4), "labels_equal": eq,
                      "plain_gteps": round(m / (p_ms * 1e-3) / 1e9, 3),
-                     "learned_gteps": round(m / (l_ms * 1e-3) / 1e9, 3)}
+                     "learned_gteps": round(m / (l_ms * 1e-3) / 1e9, 3),
+                     "tie_break_ceiling": {"other_salts_ms": salts, "best_ms": min(salts),
+                                           "median_ms": float(np.median(salts)),
+                                           "best_speedup_over_plain": round(p_ms / min(salts), 4)}}
     return out
 
 

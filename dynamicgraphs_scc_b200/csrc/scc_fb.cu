@@ -105,7 +105,7 @@ __global__ void k_pivot_key(RoundArgs a, int32_t* __restrict__ class_list, int32
                 unsigned ind = (unsigned)(__ldg(a.r_begin + v + 1) - __ldg(a.r_begin + v));
                 unsigned long long prod = (unsigned long long)outd * ind;
                 if (prod > 0xFFFFFFFEull) prod = 0xFFFFFFFEull;
-                k = ((prod + 1ull) << 32) | pivot_hash((uint32_t)v);
+                k = ((prod + 1ull) << 32) | pivot_hash((uint32_t)v ^ a.pivot_salt);
                 deg += outd + ind;
                 dmax = max(dmax, outd + ind);
             }
@@ -135,7 +135,7 @@ __global__ void k_pivot_seed(RoundArgs a, const int32_t* __restrict__ class_list
     const int32_t nc = *class_count;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nc; i += (int64_t)gridDim.x * blockDim.x) {
         int32_t c = class_list[i];
-        seed_pivot(a, pivot_unhash((uint32_t)a.slot_key[c + 1]), c, q);
+        seed_pivot(a, (int32_t)((uint32_t)pivot_unhash((uint32_t)a.slot_key[c + 1]) ^ a.pivot_salt), c, q);
     }
 }
 
@@ -187,6 +187,7 @@ static RoundArgs round_args(const scc_graph* g, scc_state* s) {
     a.huge_deg = s->tune.huge_deg;
     a.async_keep = s->tune.async_keep;
     a.async_bail = std::max<int32_t>(8 * s->tune.async_max, 1 << 16);
+    a.pivot_salt = (uint32_t)s->tune.pivot_salt;
     return a;
 }
 

@@ -148,7 +148,7 @@ struct scc_state {
 
     // defaults from a B200 sweep on the mixed R-MAT + grid workload (fewer
     // resident warps in the drain mean less contention on its queue)
-    scc_tuning tune = {14, 24, 1 << 14, 1, 16, 1, 4096, 1 << 20, 2048};
+    scc_tuning tune = {14, 24, 1 << 14, 1, 16, 1, 4096, 1 << 20, 2048, 0};
 
     // kernel ledger (scc_state_profile): device time and algorithmic bytes of
     // the asynchronous reachability drain, timed with events on `stream`

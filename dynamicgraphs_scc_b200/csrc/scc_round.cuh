@@ -20,6 +20,7 @@ struct RoundArgs {
     int32_t huge_deg;           // top-down items above this degree go edge-parallel
     int32_t async_keep;         // items a warp keeps before sharing in the asynchronous drain
     int32_t async_bail;         // outstanding items at which the drain hands back to level steps
+    uint32_t pivot_salt;        // xor on the vertex id before the tie-break hash of the degree rule (0 = none)
 };
 
 __device__ __forceinline__ uint32_t pivot_hash(uint32_t v) {

@@ -302,6 +302,7 @@ extern "C" int scc_state_set_tuning(scc_state* s, const scc_tuning* t) {
     if (t->huge_deg > 0) s->tune.huge_deg = t->huge_deg;
     if (t->tile_min_live != 0) s->tune.tile_min_live = t->tile_min_live > 0 ? t->tile_min_live : -1;
     if (t->tile_min_span > 0) s->tune.tile_min_span = t->tile_min_span;
+    if (t->pivot_salt != 0) s->tune.pivot_salt = t->pivot_salt == -1 ? 0 : t->pivot_salt;
     return SCC_OK;
 }
 

@@ -45,6 +45,7 @@ static scc_tuning candidate(uint64_t& rng) {
     t.huge_deg = pick(K_HUGE, 3);
     t.tile_min_live = pick(K_TILE, 3);
     t.tile_min_span = pick(K_SPAN, 2);
+    t.pivot_salt = 0;
     return t;
 }
 

@@ -292,6 +292,7 @@ static RoundArgs update_round_args(const scc_graph* g, scc_state* s) {
     a.huge_deg = s->tune.huge_deg;
     a.async_keep = s->tune.async_keep;
     a.async_bail = std::max<int32_t>(8 * s->tune.async_max, 1 << 16);
+    a.pivot_salt = 0;
     return a;
 }
 

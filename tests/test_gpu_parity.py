@@ -308,3 +308,19 @@ def test_generate_compact_set_and_pivot(gpu):
     csr = O.build_csr(200, s, d)
     assert st.choose_pivot_from_color(5) == O.choose_pivot(csr, col, 5)
     assert st.choose_pivot_from_color(77) == -1
+
+
+def test_pivot_tie_break_salt_changes_speed_not_labels(gpu):
+    # other tie-breaks of the degree rule pick other equally good pivots; the
+    # decomposition must not change
+    n, s, d, csr = seeded_graph(rmat_scale=12, edge_factor=6, grid_side=96, seed=41)
+    exp = O.tarjan_canonical(csr[0], csr[1])
+    g = Graph.from_edges(n, s, d)
+    st = State(g)
+    for salt in (7, 123456, -1):
+        st.set_tuning(pivot_salt=salt)
+        st.reset()
+        st.run(2)
+        assert np.array_equal(st.canonical_labels(), exp), salt
+    assert st.get_tuning()["pivot_salt"] == 0
+    st.free(); g.free()
