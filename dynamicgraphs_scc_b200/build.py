@@ -22,6 +22,7 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = [
     "scc_graph.cu",
+    "scc_sort.cu",
     "scc_state.cu",
     "scc_trim.cu",
     "scc_fb.cu",

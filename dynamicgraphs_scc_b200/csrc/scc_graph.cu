@@ -7,8 +7,7 @@
 // sort of (dst<<32 | src) gives the transpose sorted by source.  Offsets are
 // filled from the sorted keys by a gap-fill kernel.  Duplicates and self-loops
 // are kept unless the caller asks otherwise, as gm_graph keeps them.
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_select.cuh>
+#include "scc_sort.cuh"
 #include <stdarg.h>
 #include <stdlib.h>
 #include <string.h>
@@ -163,7 +162,7 @@ static int build_side(int32_t n, int64_t m, const int32_t* hi, const int32_t* lo
     // temporaries come from the library's pool, stream-ordered on st (no
     // device-wide cudaMalloc/cudaFree of GB-sized key buffers per build)
     int64_t mm = m > 0 ? m : 1;
-    AsyncScratch keys_b(st), keys2_b(st), dropped_b(st), tmp_b(st), tmp2_b(st), num_b(st);
+    AsyncScratch keys_b(st), keys2_b(st), dropped_b(st);
     SCC_CUDA(keys_b.alloc(sizeof(unsigned long long) * mm));
     SCC_CUDA(keys2_b.alloc(sizeof(unsigned long long) * mm));
     SCC_CUDA(dropped_b.alloc(sizeof(unsigned long long) * 2));
@@ -178,28 +177,17 @@ static int build_side(int32_t n, int64_t m, const int32_t* hi, const int32_t* lo
     }
     int end_bit = 32 + bits_for(n + 1);
     if (drop_self) end_bit = 64;
-    size_t tmp_bytes = 0;
-    cub::DoubleBuffer<unsigned long long> db(keys, keys2);
-    SCC_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, (int)m, 0, end_bit, st));
-    SCC_CUDA(tmp_b.alloc(tmp_bytes));
-    if (m > 0) SCC_CUDA(cub::DeviceRadixSort::SortKeys(tmp_b.p, tmp_bytes, db, (int)m, 0, end_bit, st));
-    unsigned long long* sorted = db.Current();
-    unsigned long long* other = db.Alternate();
+    SCC_TRY(scc_impl_sort_keys_u64(keys, keys2, m, end_bit, st));
+    unsigned long long* sorted = keys2;
+    unsigned long long* other = keys;
     unsigned long long h_dropped = 0;
     SCC_CUDA(cudaMemcpyAsync(&h_dropped, dropped, sizeof(h_dropped), cudaMemcpyDeviceToHost, st));
     SCC_CUDA(cudaStreamSynchronize(st));
     int64_t mk = m - (int64_t)h_dropped;   // self-loops sorted to the end
     if ((flags & SCC_BUILD_DEDUP) && mk > 0) {
-        SCC_CUDA(num_b.alloc(sizeof(int)));
-        int* d_num = (int*)num_b.p;
-        tmp_bytes = 0;
-        SCC_CUDA(cub::DeviceSelect::Unique(nullptr, tmp_bytes, sorted, other, d_num, (int)mk, st));
-        SCC_CUDA(tmp2_b.alloc(tmp_bytes));
-        SCC_CUDA(cub::DeviceSelect::Unique(tmp2_b.p, tmp_bytes, sorted, other, d_num, (int)mk, st));
-        int h_num = 0;
-        SCC_CUDA(cudaMemcpyAsync(&h_num, d_num, sizeof(int), cudaMemcpyDeviceToHost, st));
-        SCC_CUDA(cudaStreamSynchronize(st));
-        mk = h_num;
+        int64_t mu = 0;
+        SCC_TRY(scc_impl_unique_u64(sorted, other, mk, &mu, st));
+        mk = mu;
         unsigned long long* t = sorted; sorted = other; other = t;
     }
     int32_t *begin = nullptr, *idx = nullptr;
@@ -263,17 +251,13 @@ static int transpose_into(scc_graph* g, cudaStream_t st) {
         SCC_CUDA(cudaMemsetAsync(g->r_begin, 0, sizeof(int32_t) * ((size_t)n + 1), st));
         return SCC_OK;
     }
-    AsyncScratch src(st), keys(st), tmp(st);
+    AsyncScratch src(st), keys(st);
     SCC_CUDA(src.alloc(sizeof(int32_t) * (size_t)m));
     SCC_CUDA(keys.alloc(sizeof(int32_t) * (size_t)m));
     k_expand_sources<<<scc_blocks((int64_t)n * 32, 256, 148 * 64), 256, 0, st>>>(n, g->begin, (int32_t*)src.p);
     SCC_CUDA(cudaPeekAtLastError());
-    size_t tb = 0;
-    SCC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, g->node_idx, (int32_t*)keys.p, (const int32_t*)src.p,
-                                             g->r_node_idx, (int)m, 0, bits_for(n), st));
-    SCC_CUDA(tmp.alloc(tb));
-    SCC_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, g->node_idx, (int32_t*)keys.p, (const int32_t*)src.p,
-                                             g->r_node_idx, (int)m, 0, bits_for(n), st));
+    SCC_TRY(scc_impl_sort_pairs_u32(reinterpret_cast<const uint32_t*>(g->node_idx), (uint32_t*)keys.p,
+                                    (const int32_t*)src.p, g->r_node_idx, m, bits_for(n), st));
     SCC_CUDA(fill_offsets(m, n, (const int32_t*)keys.p, g->r_begin, st));
     return SCC_OK;
 }
@@ -470,25 +454,19 @@ static int upload_pipelined(scc_graph* g, const int32_t* begin, const int32_t* n
         if (sv[j] < sv[j - 1]) sv[j] = sv[j - 1];
         if (sv[j] > n) sv[j] = n;
     }
-    int64_t biggest = 0;
     for (int j = 0; j <= UPLOAD_RUNS; ++j) rb.e[j] = begin[sv[j]];
-    for (int j = 0; j < UPLOAD_RUNS; ++j) biggest = std::max<int64_t>(biggest, rb.e[j + 1] - rb.e[j]);
     SCC_REQUIRE(rb.e[UPLOAD_RUNS] == m && rb.e[0] == 0, SCC_ERR_INVALID, "CSR offsets do not run from 0 to m");
 
     Events evs;
     SCC_CUDA(cudaStreamCreateWithFlags(&evs.cs, cudaStreamNonBlocking));
     for (auto& e : evs.ev) SCC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    AsyncScratch src(st), keys(st), vals(st), off(st), tmp(st);
+    AsyncScratch src(st), keys(st), vals(st), off(st);
     JoinOnExit join{st, evs};
     SCC_CUDA(src.alloc(sizeof(int32_t) * (size_t)m));
     SCC_CUDA(keys.alloc(sizeof(int32_t) * (size_t)m));
     SCC_CUDA(vals.alloc(sizeof(int32_t) * (size_t)m));
     SCC_CUDA(off.alloc(sizeof(int32_t) * (size_t)UPLOAD_RUNS * ((size_t)n + 1)));
     const int bits = bits_for(n);
-    size_t tb = 0;
-    SCC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, g->node_idx, (int32_t*)keys.p, (const int32_t*)src.p,
-                                             (int32_t*)vals.p, (int)biggest, 0, bits, evs.cs));
-    SCC_CUDA(tmp.alloc(tb));
     SCC_CUDA(cudaMemcpyAsync(g->begin, begin, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, st));
     for (int j = 0; j < UPLOAD_RUNS; ++j) {
         const int64_t e0 = rb.e[j], c = rb.e[j + 1] - e0;
@@ -509,10 +487,8 @@ static int upload_pipelined(scc_graph* g, const int32_t* begin, const int32_t* n
         k_expand_sources_range<<<scc_blocks((int64_t)(sv[j + 1] - sv[j]) * 32, 256, 148 * 64), 256, 0, evs.cs>>>(
             sv[j], sv[j + 1], g->begin, (int32_t*)src.p);
         SCC_CUDA(cudaPeekAtLastError());
-        size_t tbj = tb;
-        SCC_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tbj, g->node_idx + e0, (int32_t*)keys.p + e0,
-                                                 (const int32_t*)src.p + e0, (int32_t*)vals.p + e0, (int)c, 0, bits,
-                                                 evs.cs));
+        SCC_TRY(scc_impl_sort_pairs_u32(reinterpret_cast<const uint32_t*>(g->node_idx + e0), (uint32_t*)keys.p + e0,
+                                        (const int32_t*)src.p + e0, (int32_t*)vals.p + e0, c, bits, evs.cs));
         SCC_CUDA(fill_offsets(c, n, (const int32_t*)keys.p + e0, oj, evs.cs));
     }
     k_runs_begin<<<scc_blocks((int64_t)n + 1, 256, 148 * 64), 256, 0, evs.cs>>>(n, offp, g->r_begin);

@@ -1,0 +1,298 @@
+// Device sorting for CSR construction: a stable least-significant-digit radix
+// sort of 32- or 64-bit keys with optional int32 values, and the removal of
+// repeated keys from a sorted array.  gm_graph builds its CSR by sorting each
+// adjacency list (do_semi_sort, gm_graph/src/gm_graph.cc:385-420) and its
+// transpose by scattering edges in source order (make_reverse_edges,
+// :193-287); on the device both become one sort of packed keys.
+//
+// Each pass handles 8 bits.  Tiles of 4,096 elements (256 threads x 16
+// elements, striped so that a round of 256 consecutive elements is one
+// element per thread in thread order):
+//  1. k_rs_hist: a shared-memory histogram of the digit per tile, written
+//     digit-major (counts[digit * tiles + tile]);
+//  2. an exclusive scan of those counts gives every (digit, tile) its first
+//     output position;
+//  3. k_rs_scatter: each tile walks its 16 rounds in order; inside a round an
+//     element's position is its digit's running position plus the elements of
+//     that digit in earlier warps (per-warp counts in shared memory) plus the
+//     earlier lanes of its warp with that digit (__match_any_sync).  Elements
+//     leave in input order within each digit, so the sort is stable.
+#include "scc_internal.cuh"
+#include "scc_sort.cuh"
+
+#define RS_THREADS 256
+#define RS_ITEMS 16
+#define RS_TILE (RS_THREADS * RS_ITEMS)
+#define RS_BINS 256
+#define RS_WARPS (RS_THREADS / 32)
+#define SCAN_CHUNK 4096
+
+// ------------------------------------------------------------------ exclusive scan (int32, in place)
+__device__ __forceinline__ int32_t warp_incl(int32_t x) {
+    int lane = threadIdx.x & 31;
+    for (int o = 1; o < 32; o <<= 1) {
+        int32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// Exclusive prefix of one value per thread over a 256-thread block; *total = the sum.
+__device__ __forceinline__ int32_t block_excl256(int32_t x, int32_t* s_w, int32_t* total) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int32_t inc = warp_incl(x);
+    if (lane == 31) s_w[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        int32_t w = lane < RS_WARPS ? s_w[lane] : 0;
+        w = warp_incl(w);
+        if (lane < RS_WARPS) s_w[lane] = w;
+    }
+    __syncthreads();
+    int32_t r = (wid ? s_w[wid - 1] : 0) + inc - x;
+    *total = s_w[RS_WARPS - 1];
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_reduce(const int32_t* __restrict__ a, int64_t L, int32_t* __restrict__ sums) {
+    __shared__ int32_t s_w[RS_WARPS];
+    int64_t base = (int64_t)blockIdx.x * SCAN_CHUNK;
+    int32_t x = 0;
+    for (int r = 0; r < SCAN_CHUNK / RS_THREADS; ++r) {
+        int64_t i = base + r * RS_THREADS + threadIdx.x;
+        if (i < L) x += a[i];
+    }
+    int32_t tot = 0;
+    block_excl256(x, s_w, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+// One block: exclusive scan of the chunk sums, in place.
+__global__ void k_scan_top(int32_t* __restrict__ sums, int32_t nb) {
+    __shared__ int32_t s_w[RS_WARPS];
+    int32_t carry = 0;
+    for (int32_t b0 = 0; b0 < nb; b0 += RS_THREADS) {
+        int32_t i = b0 + threadIdx.x;
+        int32_t x = i < nb ? sums[i] : 0;
+        int32_t tot = 0;
+        int32_t e = block_excl256(x, s_w, &tot);
+        if (i < nb) sums[i] = carry + e;
+        carry += tot;
+    }
+}
+
+__global__ void k_scan_down(int32_t* __restrict__ a, int64_t L, const int32_t* __restrict__ sums) {
+    __shared__ int32_t s_w[RS_WARPS];
+    int64_t base = (int64_t)blockIdx.x * SCAN_CHUNK;
+    int32_t run = sums[blockIdx.x];
+    for (int r = 0; r < SCAN_CHUNK / RS_THREADS; ++r) {
+        int64_t i = base + r * RS_THREADS + threadIdx.x;
+        int32_t x = i < L ? a[i] : 0;
+        int32_t tot = 0;
+        int32_t e = block_excl256(x, s_w, &tot);
+        if (i < L) a[i] = run + e;
+        run += tot;
+    }
+}
+
+static cudaError_t scan_excl(int32_t* a, int64_t L, int32_t* sums, cudaStream_t st) {
+    int64_t nb = (L + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    if (nb == 0) return cudaSuccess;
+    k_scan_reduce<<<(unsigned)nb, RS_THREADS, 0, st>>>(a, L, sums);
+    k_scan_top<<<1, RS_THREADS, 0, st>>>(sums, (int32_t)nb);
+    k_scan_down<<<(unsigned)nb, RS_THREADS, 0, st>>>(a, L, sums);
+    return cudaPeekAtLastError();
+}
+
+// ------------------------------------------------------------------ radix passes
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K* __restrict__ keys, int64_t m, int shift,
+                                                        int32_t ntiles, int32_t* __restrict__ counts) {
+    __shared__ int32_t h[RS_BINS];
+    for (int32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        h[threadIdx.x] = 0;
+        __syncthreads();
+        int64_t base = (int64_t)tile * RS_TILE;
+        for (int r = 0; r < RS_ITEMS; ++r) {
+            int64_t i = base + r * RS_THREADS + threadIdx.x;
+            if (i < m) atomicAdd(&h[(unsigned)(keys[i] >> shift) & (RS_BINS - 1)], 1);
+        }
+        __syncthreads();
+        counts[(int64_t)threadIdx.x * ntiles + tile] = h[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+template <typename K, bool VALS>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__ kin, K* __restrict__ kout,
+                                                           const int32_t* __restrict__ vin,
+                                                           int32_t* __restrict__ vout, int64_t m, int shift,
+                                                           int32_t ntiles, const int32_t* __restrict__ offs) {
+    __shared__ int32_t run[RS_BINS];
+    __shared__ int32_t wcnt[RS_WARPS][RS_BINS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int j = threadIdx.x; j < RS_WARPS * RS_BINS; j += RS_THREADS) (&wcnt[0][0])[j] = 0;
+    for (int32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        run[threadIdx.x] = offs[(int64_t)threadIdx.x * ntiles + tile];
+        __syncthreads();
+        int64_t base = (int64_t)tile * RS_TILE;
+        for (int r = 0; r < RS_ITEMS; ++r) {
+            int64_t i = base + r * RS_THREADS + threadIdx.x;
+            bool valid = i < m;
+            K k = valid ? kin[i] : (K)0;
+            int32_t v = (VALS && valid) ? vin[i] : 0;
+            int d = valid ? (int)((unsigned)(k >> shift) & (RS_BINS - 1)) : RS_BINS + lane;   // invalid lanes match nobody
+            unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
+            int lr = __popc(peers & ((1u << lane) - 1u));
+            bool leader = lane == __ffs(peers) - 1;
+            if (valid && leader) wcnt[wid][d] = __popc(peers);
+            __syncthreads();
+            if (valid) {
+                int32_t pre = 0;
+                for (int w = 0; w < wid; ++w) pre += wcnt[w][d];
+                int64_t pos = (int64_t)run[d] + pre + lr;
+                kout[pos] = k;
+                if (VALS) vout[pos] = v;
+            }
+            __syncthreads();
+            if (valid && leader) {
+                atomicAdd(&run[d], __popc(peers));
+                wcnt[wid][d] = 0;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <typename K>
+static int radix_sort(const K* keys_in, K* keys_out, const int32_t* vals_in, int32_t* vals_out, int64_t m,
+                      int bits, cudaStream_t st) {
+    SCC_REQUIRE(m >= 0 && m < (1LL << 31), SCC_ERR_INVALID, "sort of %lld elements", (long long)m);
+    const bool vals = vals_in != nullptr;
+    if (m == 0) return SCC_OK;
+    const int passes = (bits + 7) / 8;
+    if (passes == 0) {
+        SCC_CUDA(cudaMemcpyAsync(keys_out, keys_in, sizeof(K) * (size_t)m, cudaMemcpyDeviceToDevice, st));
+        if (vals) SCC_CUDA(cudaMemcpyAsync(vals_out, vals_in, sizeof(int32_t) * (size_t)m, cudaMemcpyDeviceToDevice, st));
+        return SCC_OK;
+    }
+    const int32_t ntiles = (int32_t)((m + RS_TILE - 1) / RS_TILE);
+    const int64_t L = (int64_t)RS_BINS * ntiles;
+    void *kt = nullptr, *vt = nullptr, *cnt = nullptr, *sums = nullptr;
+    int rc = SCC_OK;
+    cudaError_t e = scc_impl_malloc_async(&kt, sizeof(K) * (size_t)m, st);
+    if (e == cudaSuccess && vals) e = scc_impl_malloc_async(&vt, sizeof(int32_t) * (size_t)m, st);
+    if (e == cudaSuccess) e = scc_impl_malloc_async(&cnt, sizeof(int32_t) * (size_t)L, st);
+    if (e == cudaSuccess) e = scc_impl_malloc_async(&sums, sizeof(int32_t) * (size_t)((L + SCAN_CHUNK - 1) / SCAN_CHUNK + 1), st);
+    if (e == cudaSuccess) {
+        // the last pass must write keys_out: start in keys_out when the pass count is odd
+        const K* ksrc = keys_in;
+        const int32_t* vsrc = vals_in;
+        K* kbuf[2] = {keys_out, (K*)kt};
+        int32_t* vbuf[2] = {vals_out, (int32_t*)vt};
+        int cur = (passes & 1) ? 0 : 1;
+        unsigned blocks = (unsigned)std::min<int32_t>(ntiles, 148 * 8);
+        for (int p = 0; p < passes && e == cudaSuccess; ++p) {
+            int shift = 8 * p;
+            k_rs_hist<K><<<blocks, RS_THREADS, 0, st>>>(ksrc, m, shift, ntiles, (int32_t*)cnt);
+            e = cudaPeekAtLastError();
+            if (e == cudaSuccess) e = scan_excl((int32_t*)cnt, L, (int32_t*)sums, st);
+            if (e != cudaSuccess) break;
+            if (vals)
+                k_rs_scatter<K, true><<<blocks, RS_THREADS, 0, st>>>(ksrc, kbuf[cur], vsrc, vbuf[cur], m, shift,
+                                                                    ntiles, (const int32_t*)cnt);
+            else
+                k_rs_scatter<K, false><<<blocks, RS_THREADS, 0, st>>>(ksrc, kbuf[cur], nullptr, nullptr, m, shift,
+                                                                     ntiles, (const int32_t*)cnt);
+            e = cudaPeekAtLastError();
+            ksrc = kbuf[cur];
+            vsrc = vbuf[cur];
+            cur ^= 1;
+        }
+    }
+    if (e != cudaSuccess) rc = scc_cuda_status(e, "radix sort", __FILE__, __LINE__);
+    if (kt) cudaFreeAsync(kt, st);
+    if (vt) cudaFreeAsync(vt, st);
+    if (cnt) cudaFreeAsync(cnt, st);
+    if (sums) cudaFreeAsync(sums, st);
+    return rc;
+}
+
+int scc_impl_sort_pairs_u32(const uint32_t* keys_in, uint32_t* keys_out, const int32_t* vals_in, int32_t* vals_out,
+                            int64_t m, int bits, cudaStream_t st) {
+    return radix_sort<uint32_t>(keys_in, keys_out, vals_in, vals_out, m, bits, st);
+}
+
+int scc_impl_sort_keys_u64(const unsigned long long* keys_in, unsigned long long* keys_out, int64_t m, int bits,
+                           cudaStream_t st) {
+    return radix_sort<unsigned long long>(keys_in, keys_out, nullptr, nullptr, m, bits, st);
+}
+
+// ------------------------------------------------------------------ unique of a sorted array
+// Per tile the kept elements (first of each run of equal keys) are counted,
+// the counts scanned, and each tile writes its kept elements in order.
+__global__ void k_uniq_count(const unsigned long long* __restrict__ a, int64_t m, int32_t ntiles,
+                             int32_t* __restrict__ counts) {
+    __shared__ int32_t s_w[RS_WARPS];
+    for (int32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int64_t base = (int64_t)tile * RS_TILE;
+        int32_t c = 0;
+        for (int r = 0; r < RS_ITEMS; ++r) {
+            int64_t i = base + r * RS_THREADS + threadIdx.x;
+            if (i < m && (i == 0 || a[i] != a[i - 1])) ++c;
+        }
+        int32_t tot = 0;
+        block_excl256(c, s_w, &tot);
+        if (threadIdx.x == 0) counts[tile] = tot;
+    }
+}
+
+__global__ void k_uniq_write(const unsigned long long* __restrict__ a, unsigned long long* __restrict__ out,
+                             int64_t m, int32_t ntiles, const int32_t* __restrict__ offs) {
+    __shared__ int32_t s_w[RS_WARPS];
+    for (int32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int64_t base = (int64_t)tile * RS_TILE;
+        int32_t run = offs[tile];
+        for (int r = 0; r < RS_ITEMS; ++r) {
+            int64_t i = base + r * RS_THREADS + threadIdx.x;
+            bool keep = i < m && (i == 0 || a[i] != a[i - 1]);
+            int32_t tot = 0;
+            int32_t e = block_excl256(keep ? 1 : 0, s_w, &tot);
+            if (keep) out[(int64_t)run + e] = a[i];
+            run += tot;
+        }
+    }
+}
+
+int scc_impl_unique_u64(const unsigned long long* a, unsigned long long* out, int64_t m, int64_t* m_out,
+                        cudaStream_t st) {
+    *m_out = 0;
+    if (m <= 0) return SCC_OK;
+    SCC_REQUIRE(m < (1LL << 31), SCC_ERR_INVALID, "unique of %lld elements", (long long)m);
+    const int32_t ntiles = (int32_t)((m + RS_TILE - 1) / RS_TILE);
+    void *cnt = nullptr, *sums = nullptr;
+    SCC_CUDA(scc_impl_malloc_async(&cnt, sizeof(int32_t) * ((size_t)ntiles + 1), st));
+    cudaError_t e = scc_impl_malloc_async(&sums, sizeof(int32_t) * ((size_t)ntiles / SCAN_CHUNK + 2), st);
+    int32_t total = 0;
+    if (e == cudaSuccess) {
+        unsigned blocks = (unsigned)std::min<int32_t>(ntiles, 148 * 8);
+        k_uniq_count<<<blocks, RS_THREADS, 0, st>>>(a, m, ntiles, (int32_t*)cnt);
+        e = cudaPeekAtLastError();
+        // one extra zero entry after the tiles: its exclusive prefix is the total
+        if (e == cudaSuccess) e = cudaMemsetAsync((int32_t*)cnt + ntiles, 0, sizeof(int32_t), st);
+        if (e == cudaSuccess) e = scan_excl((int32_t*)cnt, (int64_t)ntiles + 1, (int32_t*)sums, st);
+        if (e == cudaSuccess) {
+            k_uniq_write<<<blocks, RS_THREADS, 0, st>>>(a, out, m, ntiles, (const int32_t*)cnt);
+            e = cudaPeekAtLastError();
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&total, (int32_t*)cnt + ntiles, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (cnt) cudaFreeAsync(cnt, st);
+    if (sums) cudaFreeAsync(sums, st);
+    if (e != cudaSuccess) return scc_cuda_status(e, "unique", __FILE__, __LINE__);
+    *m_out = total;
+    return SCC_OK;
+}
