@@ -351,6 +351,7 @@ extern "C" int scc_graph_upload_csr(scc_graph* g, const int32_t* begin, const in
     cudaStream_t st = (cudaStream_t)stream;
     size_t nb = sizeof(int32_t) * ((size_t)g->n + 1), mb = sizeof(int32_t) * (size_t)g->m;
     g->self_loops = -1;                      // new contents: count again when needed
+    g->rec_valid = false;
     SCC_CUDA(cudaMemcpyAsync(g->begin, begin, nb, cudaMemcpyHostToDevice, st));
     SCC_CUDA(cudaMemcpyAsync(g->r_begin, r_begin, nb, cudaMemcpyHostToDevice, st));
     if (g->m > 0) {
@@ -445,6 +446,7 @@ static int upload_pipelined(scc_graph* g, const int32_t* begin, const int32_t* n
     // the final byte.
     static const int cut_percent[UPLOAD_RUNS - 1] = {45, 75, 92};
     RunBounds rb;
+    int64_t biggest = 0;
     int32_t sv[UPLOAD_RUNS + 1];
     sv[0] = 0;
     sv[UPLOAD_RUNS] = n;
@@ -455,17 +457,21 @@ static int upload_pipelined(scc_graph* g, const int32_t* begin, const int32_t* n
         if (sv[j] > n) sv[j] = n;
     }
     for (int j = 0; j <= UPLOAD_RUNS; ++j) rb.e[j] = begin[sv[j]];
+    for (int j = 0; j < UPLOAD_RUNS; ++j) biggest = std::max<int64_t>(biggest, rb.e[j + 1] - rb.e[j]);
     SCC_REQUIRE(rb.e[UPLOAD_RUNS] == m && rb.e[0] == 0, SCC_ERR_INVALID, "CSR offsets do not run from 0 to m");
 
     Events evs;
     SCC_CUDA(cudaStreamCreateWithFlags(&evs.cs, cudaStreamNonBlocking));
     for (auto& e : evs.ev) SCC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    AsyncScratch src(st), keys(st), vals(st), off(st);
+    AsyncScratch src(st), keys(st), vals(st), off(st), sort_tmp(st);
     JoinOnExit join{st, evs};
     SCC_CUDA(src.alloc(sizeof(int32_t) * (size_t)m));
     SCC_CUDA(keys.alloc(sizeof(int32_t) * (size_t)m));
     SCC_CUDA(vals.alloc(sizeof(int32_t) * (size_t)m));
     SCC_CUDA(off.alloc(sizeof(int32_t) * (size_t)UPLOAD_RUNS * ((size_t)n + 1)));
+    // every scratch buffer is taken before the first copy, so a failed
+    // allocation leaves the graph as it was
+    SCC_CUDA(sort_tmp.alloc(scc_impl_sort_scratch_bytes(biggest, sizeof(int32_t), true)));
     const int bits = bits_for(n);
     SCC_CUDA(cudaMemcpyAsync(g->begin, begin, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, st));
     for (int j = 0; j < UPLOAD_RUNS; ++j) {
@@ -488,7 +494,8 @@ static int upload_pipelined(scc_graph* g, const int32_t* begin, const int32_t* n
             sv[j], sv[j + 1], g->begin, (int32_t*)src.p);
         SCC_CUDA(cudaPeekAtLastError());
         SCC_TRY(scc_impl_sort_pairs_u32(reinterpret_cast<const uint32_t*>(g->node_idx + e0), (uint32_t*)keys.p + e0,
-                                        (const int32_t*)src.p + e0, (int32_t*)vals.p + e0, c, bits, evs.cs));
+                                        (const int32_t*)src.p + e0, (int32_t*)vals.p + e0, c, bits, evs.cs,
+                                        sort_tmp.p));
         SCC_CUDA(fill_offsets(c, n, (const int32_t*)keys.p + e0, oj, evs.cs));
     }
     k_runs_begin<<<scc_blocks((int64_t)n + 1, 256, 148 * 64), 256, 0, evs.cs>>>(n, offp, g->r_begin);
@@ -505,6 +512,7 @@ extern "C" int scc_graph_upload_csr_out(scc_graph* g, const int32_t* begin, cons
     SCC_CUDA(cudaSetDevice(g->device));
     cudaStream_t st = (cudaStream_t)stream;
     g->self_loops = -1;                      // new contents: count again when needed
+    g->rec_valid = false;
     if (g->m >= UPLOAD_PIPELINE_MIN_EDGES) return upload_pipelined(g, begin, node_idx, st);
     SCC_CUDA(cudaMemcpyAsync(g->begin, begin, sizeof(int32_t) * ((size_t)g->n + 1), cudaMemcpyHostToDevice, st));
     if (g->m > 0)
@@ -518,6 +526,7 @@ extern "C" int scc_graph_free(scc_graph* g) {
     if (g->owns) {
         cudaFree(g->begin); cudaFree(g->node_idx); cudaFree(g->r_begin); cudaFree(g->r_node_idx);
     }
+    cudaFree(g->rec);
     delete g;
     return SCC_OK;
 }

@@ -165,9 +165,24 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__
     }
 }
 
+static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Scratch of one sort: the alternate key and value buffers, the per-(digit,
+// tile) counts and the scan's chunk sums.
+static size_t sort_scratch(int64_t m, size_t key_bytes, bool vals) {
+    const int64_t ntiles = (m + RS_TILE - 1) / RS_TILE;
+    const int64_t L = (int64_t)RS_BINS * ntiles;
+    return align256(key_bytes * (size_t)m) + (vals ? align256(sizeof(int32_t) * (size_t)m) : 0) +
+           align256(sizeof(int32_t) * (size_t)L) + align256(sizeof(int32_t) * (size_t)(L / SCAN_CHUNK + 2));
+}
+
+size_t scc_impl_sort_scratch_bytes(int64_t m, size_t key_bytes, bool vals) {
+    return sort_scratch(m > 0 ? m : 1, key_bytes, vals);
+}
+
 template <typename K>
 static int radix_sort(const K* keys_in, K* keys_out, const int32_t* vals_in, int32_t* vals_out, int64_t m,
-                      int bits, cudaStream_t st) {
+                      int bits, cudaStream_t st, void* scratch) {
     SCC_REQUIRE(m >= 0 && m < (1LL << 31), SCC_ERR_INVALID, "sort of %lld elements", (long long)m);
     const bool vals = vals_in != nullptr;
     if (m == 0) return SCC_OK;
@@ -179,32 +194,39 @@ static int radix_sort(const K* keys_in, K* keys_out, const int32_t* vals_in, int
     }
     const int32_t ntiles = (int32_t)((m + RS_TILE - 1) / RS_TILE);
     const int64_t L = (int64_t)RS_BINS * ntiles;
-    void *kt = nullptr, *vt = nullptr, *cnt = nullptr, *sums = nullptr;
+    void* own = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (!scratch) {
+        e = scc_impl_malloc_async(&own, sort_scratch(m, sizeof(K), vals), st);
+        scratch = own;
+    }
     int rc = SCC_OK;
-    cudaError_t e = scc_impl_malloc_async(&kt, sizeof(K) * (size_t)m, st);
-    if (e == cudaSuccess && vals) e = scc_impl_malloc_async(&vt, sizeof(int32_t) * (size_t)m, st);
-    if (e == cudaSuccess) e = scc_impl_malloc_async(&cnt, sizeof(int32_t) * (size_t)L, st);
-    if (e == cudaSuccess) e = scc_impl_malloc_async(&sums, sizeof(int32_t) * (size_t)((L + SCAN_CHUNK - 1) / SCAN_CHUNK + 1), st);
     if (e == cudaSuccess) {
+        char* p = (char*)scratch;
+        K* kt = (K*)p;                     p += align256(sizeof(K) * (size_t)m);
+        int32_t* vt = nullptr;
+        if (vals) { vt = (int32_t*)p;      p += align256(sizeof(int32_t) * (size_t)m); }
+        int32_t* cnt = (int32_t*)p;        p += align256(sizeof(int32_t) * (size_t)L);
+        int32_t* sums = (int32_t*)p;
         // the last pass must write keys_out: start in keys_out when the pass count is odd
         const K* ksrc = keys_in;
         const int32_t* vsrc = vals_in;
-        K* kbuf[2] = {keys_out, (K*)kt};
-        int32_t* vbuf[2] = {vals_out, (int32_t*)vt};
+        K* kbuf[2] = {keys_out, kt};
+        int32_t* vbuf[2] = {vals_out, vt};
         int cur = (passes & 1) ? 0 : 1;
         unsigned blocks = (unsigned)std::min<int32_t>(ntiles, 148 * 8);
-        for (int p = 0; p < passes && e == cudaSuccess; ++p) {
-            int shift = 8 * p;
-            k_rs_hist<K><<<blocks, RS_THREADS, 0, st>>>(ksrc, m, shift, ntiles, (int32_t*)cnt);
+        for (int p2 = 0; p2 < passes && e == cudaSuccess; ++p2) {
+            int shift = 8 * p2;
+            k_rs_hist<K><<<blocks, RS_THREADS, 0, st>>>(ksrc, m, shift, ntiles, cnt);
             e = cudaPeekAtLastError();
-            if (e == cudaSuccess) e = scan_excl((int32_t*)cnt, L, (int32_t*)sums, st);
+            if (e == cudaSuccess) e = scan_excl(cnt, L, sums, st);
             if (e != cudaSuccess) break;
             if (vals)
                 k_rs_scatter<K, true><<<blocks, RS_THREADS, 0, st>>>(ksrc, kbuf[cur], vsrc, vbuf[cur], m, shift,
-                                                                    ntiles, (const int32_t*)cnt);
+                                                                    ntiles, cnt);
             else
                 k_rs_scatter<K, false><<<blocks, RS_THREADS, 0, st>>>(ksrc, kbuf[cur], nullptr, nullptr, m, shift,
-                                                                     ntiles, (const int32_t*)cnt);
+                                                                     ntiles, cnt);
             e = cudaPeekAtLastError();
             ksrc = kbuf[cur];
             vsrc = vbuf[cur];
@@ -212,21 +234,18 @@ static int radix_sort(const K* keys_in, K* keys_out, const int32_t* vals_in, int
         }
     }
     if (e != cudaSuccess) rc = scc_cuda_status(e, "radix sort", __FILE__, __LINE__);
-    if (kt) cudaFreeAsync(kt, st);
-    if (vt) cudaFreeAsync(vt, st);
-    if (cnt) cudaFreeAsync(cnt, st);
-    if (sums) cudaFreeAsync(sums, st);
+    if (own) cudaFreeAsync(own, st);
     return rc;
 }
 
 int scc_impl_sort_pairs_u32(const uint32_t* keys_in, uint32_t* keys_out, const int32_t* vals_in, int32_t* vals_out,
-                            int64_t m, int bits, cudaStream_t st) {
-    return radix_sort<uint32_t>(keys_in, keys_out, vals_in, vals_out, m, bits, st);
+                            int64_t m, int bits, cudaStream_t st, void* scratch) {
+    return radix_sort<uint32_t>(keys_in, keys_out, vals_in, vals_out, m, bits, st, scratch);
 }
 
 int scc_impl_sort_keys_u64(const unsigned long long* keys_in, unsigned long long* keys_out, int64_t m, int bits,
                            cudaStream_t st) {
-    return radix_sort<unsigned long long>(keys_in, keys_out, nullptr, nullptr, m, bits, st);
+    return radix_sort<unsigned long long>(keys_in, keys_out, nullptr, nullptr, m, bits, st, nullptr);
 }
 
 // ------------------------------------------------------------------ unique of a sorted array

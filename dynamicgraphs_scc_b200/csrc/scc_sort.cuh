@@ -5,9 +5,12 @@
 #include "scc_internal.cuh"
 
 // Sorts m (key, value) pairs by the low `bits` bits of the key, stably;
-// vals_in may be NULL (keys only).  Inputs are not modified.
+// vals_in may be NULL (keys only).  Inputs are not modified.  scratch: NULL
+// (taken from the pool) or at least scc_impl_sort_scratch_bytes(m, 4, vals)
+// bytes, 256-byte aligned, that the caller allocated beforehand.
 int scc_impl_sort_pairs_u32(const uint32_t* keys_in, uint32_t* keys_out, const int32_t* vals_in, int32_t* vals_out,
-                            int64_t m, int bits, cudaStream_t st);
+                            int64_t m, int bits, cudaStream_t st, void* scratch = nullptr);
+size_t scc_impl_sort_scratch_bytes(int64_t m, size_t key_bytes, bool vals);
 int scc_impl_sort_keys_u64(const unsigned long long* keys_in, unsigned long long* keys_out, int64_t m, int bits,
                            cudaStream_t st);
 // out = a with repeated neighbours removed; *m_out its length (synchronises st).
