@@ -19,6 +19,7 @@
 #include <algorithm>
 #include "scc_round.cuh"
 #include "scc_batch.cuh"
+#include "scc_sort.cuh"
 
 struct BatchArgs {
     const int32_t* begin; const int32_t* adj; const int32_t* rbegin; const int32_t* radj;
@@ -32,6 +33,7 @@ struct BatchArgs {
     unsigned long long* key;    // [3N] pivot key per colour
     int32_t* ctr;               // BATCH_CTR_* counters
     int32_t warp_deg;           // lists longer than this are expanded by a whole warp
+    const int32_t* members;     // class mode: unit k is members[offs[k] .. offs[k+1]); NULL: vertex ids
 };
 
 __device__ __forceinline__ int32_t b_fw_colour(int32_t p) { return 3 * p + 1; }
@@ -228,12 +230,15 @@ __device__ void b_graph(const BatchArgs& a, int32_t gi, int32_t* s) {
     int32_t* q = a.q + 2LL * lo;          // [2 ng]: peel queue (vertices | classes) or BFS items
     int32_t* live = a.live + lo;
     int32_t* live2 = a.live2 + lo;
-    const int32_t c0 = 3 * lo;
+    // one class per unit: colour 3 x its first vertex (a multiple of 3, so it
+    // never meets the 3p+1 / 3p+2 colours of a pivot's parts)
+    const int32_t c0 = 3 * (a.members ? a.members[lo] : lo);
     for (int32_t i = threadIdx.x; i < ng; i += blockDim.x) {
-        a.color[lo + i] = c0;
-        a.scc[lo + i] = SCC_NIL_NODE;
-        a.mark[lo + i] = 0;
-        live[i] = lo + i;
+        int32_t v = a.members ? a.members[lo + i] : lo + i;
+        a.color[v] = c0;
+        a.scc[v] = SCC_NIL_NODE;
+        a.mark[v] = 0;
+        live[i] = v;
     }
     int32_t nlive = ng;
     int32_t rounds = 0, levels = 0;
@@ -410,6 +415,7 @@ static int batch_enqueue(scc_batch_plan* p, int sms) {
     a.key = p->d_key;
     a.ctr = p->d_ctr;
     a.warp_deg = p->tune.warp_deg;
+    a.members = nullptr;
     SCC_CUDA(cudaMemsetAsync(p->d_ctr, 0, sizeof(int32_t) * BATCH_CTR_WORDS, s->stream));
     k_batch_scc<<<sms * p->tune.blocks_per_sm, p->tune.threads, 0, s->stream>>>(a);
     SCC_CUDA(cudaPeekAtLastError());
@@ -576,5 +582,90 @@ extern "C" int scc_batch_autotune(const scc_graph* g, scc_state* s, const int32_
     }
     if (best) *best = cand[0];
     if (best_ms) *best_ms = ms[0];
+    return SCC_OK;
+}
+
+// ------------------------------------------------------------------ the recursion's tail
+// Once few vertices are left (tail_live), every remaining class is an
+// independent subproblem: the live vertices are grouped by class (a stable
+// sort of (colour, vertex)), and one persistent launch decomposes each class
+// inside a block, as for a batch of graphs, instead of further rounds of many
+// launches and host round trips.  Classes are unions of SCCs, so the labels
+// are the same.  Skipped (nothing done) when a class is larger than
+// tail_class, which one block would take too long to finish alone.
+__global__ void k_tail_keys(const int32_t* __restrict__ live, int32_t nl, const int32_t* __restrict__ color,
+                            uint32_t* __restrict__ keys) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nl; i += (int64_t)gridDim.x * blockDim.x)
+        keys[i] = (uint32_t)color[live[i]];
+}
+
+int scc_impl_resolve_tail(const scc_graph* g, scc_state* s, bool* taken) {
+    *taken = false;
+    const int32_t nl = s->live_count;
+    if (nl <= 0) return SCC_OK;
+    cudaStream_t st = s->stream;
+    struct Pool {
+        cudaStream_t st;
+        std::vector<void*> v;
+        ~Pool() { for (void* p : v) cudaFreeAsync(p, st); }
+        cudaError_t get(void** p, size_t b) { cudaError_t e = scc_impl_malloc_async(p, b, st); if (e == cudaSuccess) v.push_back(*p); return e; }
+    } pool{st, {}};
+    uint32_t *keys = nullptr, *skeys = nullptr;
+    int32_t *members = nullptr, *starts = nullptr, *order = nullptr, *ctr = nullptr;
+    SCC_CUDA(pool.get((void**)&keys, sizeof(uint32_t) * (size_t)nl));
+    SCC_CUDA(pool.get((void**)&skeys, sizeof(uint32_t) * (size_t)nl));
+    SCC_CUDA(pool.get((void**)&members, sizeof(int32_t) * (size_t)nl));
+    SCC_CUDA(pool.get((void**)&starts, sizeof(int32_t) * ((size_t)nl + 1)));
+    k_tail_keys<<<scc_blocks(nl), SCC_THREADS, 0, st>>>(s->live, nl, s->color, keys);
+    SCC_LAUNCHED(s);
+    SCC_TRY(scc_impl_sort_pairs_u32(keys, skeys, s->live, members, nl, 32, st));
+    int64_t G = 0;
+    SCC_TRY(scc_impl_segment_starts(skeys, nl, starts, &G, st));
+    std::vector<int32_t> h((size_t)G + 1);
+    SCC_CUDA(cudaMemcpyAsync(h.data(), starts, sizeof(int32_t) * (size_t)G, cudaMemcpyDeviceToHost, st));
+    SCC_CUDA(cudaStreamSynchronize(st));
+    h[(size_t)G] = nl;
+    int32_t biggest = 0;
+    for (int64_t k = 0; k < G; ++k) biggest = std::max(biggest, h[(size_t)k + 1] - h[(size_t)k]);
+    if (biggest > s->tune.tail_class) return SCC_OK;
+    std::vector<int32_t> ord((size_t)G);
+    for (int64_t k = 0; k < G; ++k) ord[(size_t)k] = (int32_t)k;
+    std::stable_sort(ord.begin(), ord.end(), [&](int32_t x, int32_t y) { return h[x + 1] - h[x] > h[y + 1] - h[y]; });
+    if (!s->bkey) SCC_CUDA(cudaMalloc(&s->bkey, sizeof(unsigned long long) * (3 * (size_t)std::max(s->n, 1) + 3)));
+    SCC_CUDA(pool.get((void**)&order, sizeof(int32_t) * (size_t)std::max<int64_t>(G, 1)));
+    SCC_CUDA(pool.get((void**)&ctr, sizeof(int32_t) * BATCH_CTR_WORDS));
+    SCC_CUDA(cudaMemcpyAsync(starts + G, &nl, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    SCC_CUDA(cudaMemcpyAsync(order, ord.data(), sizeof(int32_t) * (size_t)G, cudaMemcpyHostToDevice, st));
+    SCC_CUDA(cudaMemsetAsync(ctr, 0, sizeof(int32_t) * BATCH_CTR_WORDS, st));
+    BatchArgs a;
+    a.begin = g->begin; a.adj = g->node_idx; a.rbegin = g->r_begin; a.radj = g->r_node_idx;
+    a.offs = starts; a.order = order; a.G = (int32_t)G;
+    a.color = s->color; a.scc = s->scc; a.mark = s->mark;
+    a.cin = reinterpret_cast<uint32_t*>(s->cnt);
+    a.cout = reinterpret_cast<uint32_t*>(s->cnt) + s->n;
+    a.q = s->qa;
+    a.live = s->live; a.live2 = s->live_tmp;
+    a.key = s->bkey;
+    a.ctr = ctr;
+    a.warp_deg = 32;
+    a.members = members;
+    int sms = 148;
+    SCC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+    k_batch_scc<<<sms * 2, 512, 0, st>>>(a);
+    SCC_LAUNCHED(s);
+    int32_t h_ctr[BATCH_CTR_WORDS];
+    SCC_CUDA(cudaMemcpyAsync(h_ctr, ctr, sizeof(h_ctr), cudaMemcpyDeviceToHost, st));
+    SCC_CUDA(cudaStreamSynchronize(st));
+    if (h_ctr[BATCH_CTR_ERROR]) {
+        scc_set_error("tail decomposition: device error %d", h_ctr[BATCH_CTR_ERROR]);
+        return h_ctr[BATCH_CTR_ERROR] == SCC_DEVERR_WAIT_LIMIT ? SCC_ERR_TIMEOUT : SCC_ERR_OOM;
+    }
+    s->fb_rounds += h_ctr[BATCH_CTR_MAX_ROUNDS];
+    s->cnt_valid = false;
+    s->live_count = 0;
+    *taken = true;
+    if (scc_trace_on())
+        fprintf(stderr, "[scc] tail: %d live vertices in %lld classes (largest %d) in one launch, up to %d rounds\n", nl,
+                (long long)G, biggest, h_ctr[BATCH_CTR_MAX_ROUNDS]);
     return SCC_OK;
 }

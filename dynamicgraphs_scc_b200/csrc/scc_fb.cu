@@ -268,6 +268,13 @@ int scc_impl_resolve_all(const scc_graph* g, scc_state* s, bool classes_split) {
     for (int round = 0; round < (1 << 30); ++round) {
         int32_t t = 0;
         int32_t classes = 0;
+        if (round >= 1 && s->tune.tail_live > 0 && s->live_count <= s->tune.tail_live &&
+            s->pivot_mode == SCC_PIVOT_DEGREE && s->log_cap == 0) {
+            // few vertices left: every class in one launch, a block per class
+            bool taken = false;
+            SCC_TRY(scc_impl_resolve_tail(g, s, &taken));
+            if (taken) break;
+        }
         if (round == 0 && classes_split) {
             // the caller peeled to the fixpoint, compacted, then split: a split
             // only recolours weakly disconnected parts, so no live vertex loses

@@ -116,6 +116,7 @@ struct scc_state {
     int32_t* tq = nullptr;           // tile drain inboxes [tq_cap], kept at -1 between uses (allocated at first use)
     int64_t tq_cap = 0;
     int32_t* tctr = nullptr;         // tile drain counters (allocated at first use)
+    unsigned long long* bkey = nullptr;  // [3n] pivot key per colour of the one-launch tail (allocated at first use)
     int32_t* block_sums = nullptr;   // scan scratch
     int32_t* ctr = nullptr;          // device counters [CTR_MAX]
     int32_t* h_ctr = nullptr;        // pinned host mirror [CTR_MAX]
@@ -153,7 +154,7 @@ struct scc_state {
 
     // defaults from a B200 sweep on the mixed R-MAT + grid workload (fewer
     // resident warps in the drain mean less contention on its queue)
-    scc_tuning tune = {14, 24, 1 << 14, 1, 16, 1, 4096, 1 << 20, 2048, 0};
+    scc_tuning tune = {14, 24, 1 << 14, 1, 16, 1, 4096, 1 << 20, 2048, 0, 1 << 20, 1 << 16};
 
     // kernel ledger (scc_state_profile): device time and algorithmic bytes of
     // the asynchronous reachability drain, timed with events on `stream`
@@ -194,6 +195,9 @@ bool scc_impl_take_wait_injection();   // consumes a pending SCC_INJECT_WAIT
 void scc_impl_pivot_release(scc_state* s);   // frees the learned-pivot and logging buffers
 // classes_split: the live classes are already weak components (a split ran last)
 int scc_impl_resolve_all(const scc_graph* g, scc_state* s, bool classes_split = false);
+// Decomposes every remaining class in one launch (a block per class); *taken is
+// false, with nothing done, when a class is above tune.tail_class vertices.
+int scc_impl_resolve_tail(const scc_graph* g, scc_state* s, bool* taken);
 int scc_impl_get_live_host(scc_state* s, std::vector<int32_t>& out);
 int scc_impl_count_colour(scc_state* s, int32_t color, int32_t* count);
 int scc_impl_build_graph_from_device_edges(int32_t n, int64_t m, const int32_t* d_src,

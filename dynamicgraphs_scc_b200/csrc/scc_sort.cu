@@ -250,9 +250,10 @@ int scc_impl_sort_keys_u64(const unsigned long long* keys_in, unsigned long long
 
 // ------------------------------------------------------------------ unique of a sorted array
 // Per tile the kept elements (first of each run of equal keys) are counted,
-// the counts scanned, and each tile writes its kept elements in order.
-__global__ void k_uniq_count(const unsigned long long* __restrict__ a, int64_t m, int32_t ntiles,
-                             int32_t* __restrict__ counts) {
+// the counts scanned, and each tile writes its kept elements in order: the
+// key itself, or (POS) its index.
+template <typename K>
+__global__ void k_uniq_count(const K* __restrict__ a, int64_t m, int32_t ntiles, int32_t* __restrict__ counts) {
     __shared__ int32_t s_w[RS_WARPS];
     for (int32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         int64_t base = (int64_t)tile * RS_TILE;
@@ -267,8 +268,9 @@ __global__ void k_uniq_count(const unsigned long long* __restrict__ a, int64_t m
     }
 }
 
-__global__ void k_uniq_write(const unsigned long long* __restrict__ a, unsigned long long* __restrict__ out,
-                             int64_t m, int32_t ntiles, const int32_t* __restrict__ offs) {
+template <typename K, typename O, bool POS>
+__global__ void k_uniq_write(const K* __restrict__ a, O* __restrict__ out, int64_t m, int32_t ntiles,
+                             const int32_t* __restrict__ offs) {
     __shared__ int32_t s_w[RS_WARPS];
     for (int32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         int64_t base = (int64_t)tile * RS_TILE;
@@ -278,14 +280,14 @@ __global__ void k_uniq_write(const unsigned long long* __restrict__ a, unsigned 
             bool keep = i < m && (i == 0 || a[i] != a[i - 1]);
             int32_t tot = 0;
             int32_t e = block_excl256(keep ? 1 : 0, s_w, &tot);
-            if (keep) out[(int64_t)run + e] = a[i];
+            if (keep) out[(int64_t)run + e] = POS ? (O)i : (O)a[i];
             run += tot;
         }
     }
 }
 
-int scc_impl_unique_u64(const unsigned long long* a, unsigned long long* out, int64_t m, int64_t* m_out,
-                        cudaStream_t st) {
+template <typename K, typename O, bool POS>
+static int uniq(const K* a, O* out, int64_t m, int64_t* m_out, cudaStream_t st) {
     *m_out = 0;
     if (m <= 0) return SCC_OK;
     SCC_REQUIRE(m < (1LL << 31), SCC_ERR_INVALID, "unique of %lld elements", (long long)m);
@@ -296,13 +298,13 @@ int scc_impl_unique_u64(const unsigned long long* a, unsigned long long* out, in
     int32_t total = 0;
     if (e == cudaSuccess) {
         unsigned blocks = (unsigned)std::min<int32_t>(ntiles, 148 * 8);
-        k_uniq_count<<<blocks, RS_THREADS, 0, st>>>(a, m, ntiles, (int32_t*)cnt);
+        k_uniq_count<K><<<blocks, RS_THREADS, 0, st>>>(a, m, ntiles, (int32_t*)cnt);
         e = cudaPeekAtLastError();
         // one extra zero entry after the tiles: its exclusive prefix is the total
         if (e == cudaSuccess) e = cudaMemsetAsync((int32_t*)cnt + ntiles, 0, sizeof(int32_t), st);
         if (e == cudaSuccess) e = scan_excl((int32_t*)cnt, (int64_t)ntiles + 1, (int32_t*)sums, st);
         if (e == cudaSuccess) {
-            k_uniq_write<<<blocks, RS_THREADS, 0, st>>>(a, out, m, ntiles, (const int32_t*)cnt);
+            k_uniq_write<K, O, POS><<<blocks, RS_THREADS, 0, st>>>(a, out, m, ntiles, (const int32_t*)cnt);
             e = cudaPeekAtLastError();
         }
         if (e == cudaSuccess)
@@ -314,4 +316,13 @@ int scc_impl_unique_u64(const unsigned long long* a, unsigned long long* out, in
     if (e != cudaSuccess) return scc_cuda_status(e, "unique", __FILE__, __LINE__);
     *m_out = total;
     return SCC_OK;
+}
+
+int scc_impl_unique_u64(const unsigned long long* a, unsigned long long* out, int64_t m, int64_t* m_out,
+                        cudaStream_t st) {
+    return uniq<unsigned long long, unsigned long long, false>(a, out, m, m_out, st);
+}
+
+int scc_impl_segment_starts(const uint32_t* keys, int64_t m, int32_t* starts, int64_t* count, cudaStream_t st) {
+    return uniq<uint32_t, int32_t, true>(keys, starts, m, count, st);
 }

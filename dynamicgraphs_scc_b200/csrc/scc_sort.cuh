@@ -16,3 +16,6 @@ int scc_impl_sort_keys_u64(const unsigned long long* keys_in, unsigned long long
 // out = a with repeated neighbours removed; *m_out its length (synchronises st).
 int scc_impl_unique_u64(const unsigned long long* a, unsigned long long* out, int64_t m, int64_t* m_out,
                         cudaStream_t st);
+// starts[j] = index where the j-th run of equal keys of a sorted array begins;
+// *count = the number of runs (synchronises st).
+int scc_impl_segment_starts(const uint32_t* keys, int64_t m, int32_t* starts, int64_t* count, cudaStream_t st);

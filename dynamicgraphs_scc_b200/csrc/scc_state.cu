@@ -223,7 +223,7 @@ extern "C" int scc_state_free(scc_state* s) {
     cudaSetDevice(s->device);
     cudaFree(s->color); cudaFree(s->scc); cudaFree(s->wcc); cudaFree(s->live); cudaFree(s->live_tmp);
     cudaFree(s->qa); cudaFree(s->qb); cudaFree(s->aq); cudaFree(s->uf); cudaFree(s->hq); cudaFree(s->hoff); cudaFree(s->cnt); cudaFree(s->ccnt); cudaFree(s->mark); cudaFree(s->aux); cudaFree(s->block_sums);
-    cudaFree(s->tq); cudaFree(s->tctr);
+    cudaFree(s->tq); cudaFree(s->tctr); cudaFree(s->bkey);
     cudaFree(s->ctr);
     if (s->h_ctr) cudaFreeHost(s->h_ctr);
     cudaFree(s->slot_key); cudaFree(s->slot_pivot); cudaFree(s->slot_fw); cudaFree(s->slot_bw); cudaFree(s->slot_count);
@@ -303,6 +303,8 @@ extern "C" int scc_state_set_tuning(scc_state* s, const scc_tuning* t) {
     if (t->tile_min_live != 0) s->tune.tile_min_live = t->tile_min_live > 0 ? t->tile_min_live : -1;
     if (t->tile_min_span > 0) s->tune.tile_min_span = t->tile_min_span;
     if (t->pivot_salt != 0) s->tune.pivot_salt = t->pivot_salt == -1 ? 0 : t->pivot_salt;
+    if (t->tail_live != 0) s->tune.tail_live = t->tail_live > 0 ? t->tail_live : -1;
+    if (t->tail_class > 0) s->tune.tail_class = t->tail_class;
     return SCC_OK;
 }
 

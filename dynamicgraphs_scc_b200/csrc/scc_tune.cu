@@ -29,6 +29,7 @@ static const int32_t K_BLOCKS[] = {1, 2};                         // drain block
 static const int32_t K_HUGE[] = {1024, 4096, 16384};              // edge-parallel hub expansion above this degree
 static const int32_t K_TILE[] = {-1, 1 << 18, 1 << 20};           // tile drain from this many live vertices
 static const int32_t K_SPAN[] = {2048, 16384};                    // smallest tile
+static const int32_t K_TAIL[] = {-1, 1 << 18, 1 << 20};           // one-launch tail from this many live vertices
 
 static scc_tuning candidate(uint64_t& rng) {
     auto pick = [&](const int32_t* v, int k) {
@@ -46,6 +47,8 @@ static scc_tuning candidate(uint64_t& rng) {
     t.tile_min_live = pick(K_TILE, 3);
     t.tile_min_span = pick(K_SPAN, 2);
     t.pivot_salt = 0;
+    t.tail_live = pick(K_TAIL, 3);
+    t.tail_class = 1 << 16;
     return t;
 }
 

@@ -180,11 +180,14 @@ typedef struct scc_tuning {
     int32_t tile_min_span;        /* smallest id range of a tile (2048) */
     int32_t pivot_salt;           /* xor on vertex ids before the degree rule's tie-break hash (0): picks
                                      another of the equally good pivots; changes speed, never labels */
+    int32_t tail_live;            /* from the second recursion round on, at most this many live vertices are
+                                     finished in one launch, a block per class (1 << 20); negative = never */
+    int32_t tail_class;           /* ... provided no class has more vertices than this (1 << 16) */
 } scc_tuning;
 int scc_state_get_tuning(scc_state* s, scc_tuning* t);
-/* Fields <= 0 keep their current value, except tile_min_live, where a negative
- * value turns the tile drain off, and pivot_salt, which any non-zero value sets
- * (and -1 resets to 0). */
+/* Fields <= 0 keep their current value, except tile_min_live and tail_live,
+ * where a negative value turns that path off, and pivot_salt, which any
+ * non-zero value sets (and -1 resets to 0). */
 int scc_state_set_tuning(scc_state* s, const scc_tuning* t);
 /* Autotuner: successive halving over the tunables with a budget of max_trials full
  * decompositions (method) of g: a seeded sample of settings (the current one among

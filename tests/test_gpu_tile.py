@@ -90,3 +90,13 @@ def test_tile_drain_hands_back_a_wide_frontier(gpu):
     s = np.concatenate([s, np.full(20, hub), nb_in]); d = np.concatenate([d, nb_out, np.full(20, hub)])
     s, d = O.dedup_edges(s, d, n=n)
     _check(n, s, d, methods=(2,), async_max=64, async_after=1)
+
+
+@pytest.mark.parametrize("tail", [dict(tail_live=-1), dict(tail_live=1 << 30, tail_class=16),
+                                  dict(tail_live=1 << 30, tail_class=1 << 20)])
+def test_recursion_tail_in_one_launch(gpu, tail):
+    # the recursion's last rounds finished by one launch with a block per
+    # class (on from the second round, off, or deferred until every class has
+    # at most 16 vertices): the labels never change
+    n, s, d, _ = seeded_graph(rmat_scale=13, edge_factor=6, grid_side=200, seed=12)
+    _check(n, s, d, methods=(0, 1, 2), tile_min_live=-1, **tail)
