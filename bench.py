@@ -522,6 +522,8 @@ def extra_c3(local_rank, steps=5, warmup=3):
         m = g.num_edges()
         st = State(g)
         st.set_pivot_model(model)
+        # both forms without the one-launch tail, which learned pivots do not use
+        st.set_tuning(tail_live=-1)
         stream = torch.cuda.ExternalStream(st.stream(), device=local_rank)
         p_ms, _ = time_steps(st, stream, steps, warmup, 0)
         p_lab = st.canonical_labels()
@@ -793,6 +795,7 @@ def main():
     st = State(g)
     if model is not None:
         st.set_pivot_model(model)
+        st.set_tuning(tail_live=-1)        # both forms without the one-launch tail, which learned pivots do not use
     pivot_mode = 1 if learned else 0
     stream = torch.cuda.ExternalStream(st.stream(), device=local_rank)
 
@@ -901,6 +904,7 @@ def main():
         st2 = State(g2)
         if learned:
             st2.set_pivot_model(model)
+            st2.set_tuning(tail_live=-1)
         pair = [(g, st), (g2, st2)]
         lab_dev = [torch.empty(n, dtype=torch.int32, device=f"cuda:{local_rank}") for _ in range(2)]
         lab_host = [torch.empty(n, dtype=torch.int32).pin_memory() for _ in range(2)]
