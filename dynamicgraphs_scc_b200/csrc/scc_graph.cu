@@ -351,7 +351,6 @@ extern "C" int scc_graph_upload_csr(scc_graph* g, const int32_t* begin, const in
     cudaStream_t st = (cudaStream_t)stream;
     size_t nb = sizeof(int32_t) * ((size_t)g->n + 1), mb = sizeof(int32_t) * (size_t)g->m;
     g->self_loops = -1;                      // new contents: count again when needed
-    g->rec_valid = false;
     SCC_CUDA(cudaMemcpyAsync(g->begin, begin, nb, cudaMemcpyHostToDevice, st));
     SCC_CUDA(cudaMemcpyAsync(g->r_begin, r_begin, nb, cudaMemcpyHostToDevice, st));
     if (g->m > 0) {
@@ -512,7 +511,6 @@ extern "C" int scc_graph_upload_csr_out(scc_graph* g, const int32_t* begin, cons
     SCC_CUDA(cudaSetDevice(g->device));
     cudaStream_t st = (cudaStream_t)stream;
     g->self_loops = -1;                      // new contents: count again when needed
-    g->rec_valid = false;
     if (g->m >= UPLOAD_PIPELINE_MIN_EDGES) return upload_pipelined(g, begin, node_idx, st);
     SCC_CUDA(cudaMemcpyAsync(g->begin, begin, sizeof(int32_t) * ((size_t)g->n + 1), cudaMemcpyHostToDevice, st));
     if (g->m > 0)
@@ -526,7 +524,6 @@ extern "C" int scc_graph_free(scc_graph* g) {
     if (g->owns) {
         cudaFree(g->begin); cudaFree(g->node_idx); cudaFree(g->r_begin); cudaFree(g->r_node_idx);
     }
-    cudaFree(g->rec);
     delete g;
     return SCC_OK;
 }

@@ -45,11 +45,6 @@ struct scc_graph {
     bool owns = true;
     bool async_arrays = false;    // arrays come from cudaMallocAsync (after an update)
     mutable int64_t self_loops = -1;  // edges u->u in the CSR; -1 = not counted yet
-    // per vertex and direction a 32-byte record {begin, end, first 6 neighbours}
-    // (the tile drain's one-load hop), built at first use, dropped when the
-    // arrays change
-    mutable int4* rec = nullptr;
-    mutable bool rec_valid = false;
 };
 
 // Device counters block (one allocation, mirrored to pinned host memory).

@@ -43,7 +43,7 @@
 #define TILE_IDLE_LIMIT (1 << 22)
 #define TILE_SLOT_LIMIT (1 << 20)
 #define TILE_BAR_LIMIT (1 << 24)
-#define TILE_SMEM_BYTES (4 * TILE_MARK_WORDS + 40 * TILE_WARPS * TILE_WBUF)
+#define TILE_SMEM_BYTES (4 * TILE_MARK_WORDS + 16 * TILE_WARPS * TILE_WBUF)
 
 struct TileArgs {
     int32_t lo;          // first vertex of tile 0 (a multiple of 16)
@@ -56,36 +56,8 @@ struct TileArgs {
     int32_t* qout;       // hand-back list of a bail (its length in CTR_QLEN)
     int64_t qcap;        // its capacity
     int32_t bail_at;
-    const int4* rec;     // per vertex and direction {begin, end, n0, n1} {n2, n3, n4, n5}
+    int32_t keep;        // items a warp keeps when it shares the rest with the block
 };
-
-#define REC_INLINE 6     // neighbours a record carries
-
-__device__ __forceinline__ const int4* rec_of(const TileArgs& t, int32_t v, int dir) {
-    return t.rec + ((int64_t)v * 4 + dir * 2);
-}
-
-__device__ __forceinline__ void prefetch_l2(const void* p) {
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
-
-// Builds the records of every vertex (both directions).
-__global__ void k_build_rec(int32_t n, const int32_t* __restrict__ begin, const int32_t* __restrict__ adj,
-                            const int32_t* __restrict__ rbegin, const int32_t* __restrict__ radj,
-                            int4* __restrict__ rec) {
-    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-        for (int dir = 0; dir < 2; ++dir) {
-            const int32_t* off = dir ? rbegin : begin;
-            const int32_t* ad = dir ? radj : adj;
-            int32_t b = off[v], e = off[v + 1];
-            int32_t x[REC_INLINE];
-#pragma unroll
-            for (int i = 0; i < REC_INLINE; ++i) x[i] = b + i < e ? ad[b + i] : -1;
-            rec[v * 4 + dir * 2] = make_int4(b, e, x[0], x[1]);
-            rec[v * 4 + dir * 2 + 1] = make_int4(x[2], x[3], x[4], x[5]);
-        }
-    }
-}
 
 __device__ __forceinline__ int32_t tld(const int32_t* p) { return *(const volatile int32_t*)p; }
 
@@ -108,10 +80,10 @@ __global__ void k_tile_seed(RoundArgs a, TileArgs t, const int32_t* __restrict__
 }
 
 struct TileList {
-    int32_t* it; int32_t* c; int32_t* r;   // this warp's list in shared memory: items, classes, records (8 ints)
-    int32_t count;                          // warp-uniform
-    int32_t pushed;                         // net change since the last publish
-    int32_t* W; int32_t* tail; int32_t* inbox; int64_t cap; int32_t* err;
+    int32_t* it; int32_t* b; int32_t* e; int32_t* c;   // this warp's list in shared memory
+    int32_t count;                                      // warp-uniform
+    int32_t pushed;                                     // net change since the last publish
+    int32_t* W; int32_t* tail; int32_t* inbox; int64_t cap; int32_t* err; int32_t keep;
     // Items beyond `keep` go to this tile's inbox (flagged: already claimed
     // here), where idle warps of the block take them.  The count is published
     // first, and the fence orders it before the items become visible.
@@ -141,18 +113,16 @@ struct TileList {
         count = keep;
         return true;
     }
-    __device__ __forceinline__ void push(bool p, int32_t item, int4 r0, int4 r1, int32_t cc) {
+    __device__ __forceinline__ void push(bool p, int32_t item, int32_t bb, int32_t ee, int32_t cc) {
         int lane = threadIdx.x & 31;
         unsigned bal = __ballot_sync(0xFFFFFFFFu, p);
         if (p) {
             int32_t pos = count + __popc(bal & ((1u << lane) - 1u));
-            it[pos] = item; c[pos] = cc;
-            int32_t* q = r + pos * 8;
-            q[0] = r0.x; q[1] = r0.y; q[2] = r0.z; q[3] = r0.w; q[4] = r1.x; q[5] = r1.y; q[6] = r1.z; q[7] = r1.w;
+            it[pos] = item; b[pos] = bb; e[pos] = ee; c[pos] = cc;
         }
         count += __popc(bal);
         pushed += __popc(bal);
-        if (count > TILE_WBUF - 32) spill(TILE_KEEP);
+        if (count > TILE_WBUF - 32) spill(keep);
     }
 };
 
@@ -208,47 +178,23 @@ __device__ __forceinline__ bool tile_send(const RoundArgs& a, const TileArgs& t,
     return __all_sync(0xFFFFFFFFu, ok);
 }
 
-// The claim of neighbour w: its mark, class and record are loaded together.
-// A new vertex of this tile starts pulling its own neighbours' classes and
-// records toward L2, so when it is expanded (usually the warp's next
-// iteration) the hop after it finds them there.
-__device__ __forceinline__ int tile_visit(const RoundArgs& a, const TileArgs& t, uint32_t* smark, int32_t lo_k,
-                                          int32_t w, int dir, int32_t c, int4& r0, int4& r1) {
-    unsigned gm = (unsigned)*(volatile uint8_t*)(a.mark + w);
-    int32_t col = __ldg(a.color + w);
-    const int4* rp = rec_of(t, w, dir);
-    r0 = __ldg(rp);
-    r1 = __ldg(rp + 1);
-    if (col != c) return 0;
-    int r = tile_claim(a, smark, lo_k, t.span, w, dir, gm);
-    if (r == 1) {
-        int32_t x[REC_INLINE] = {r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-#pragma unroll
-        for (int i = 0; i < REC_INLINE; ++i)
-            if (x[i] >= 0) { prefetch_l2(a.color + x[i]); prefetch_l2(rec_of(t, x[i], dir)); }
-    }
-    return r;
-}
-
-// Expand one item per lane (valid lanes).  rr[0] < 0: record and class not known yet.
+// Expand one item per lane (valid lanes).  b < 0: range and class not known yet.
 __device__ __forceinline__ void tile_expand(const RoundArgs& a, const TileArgs& t, uint32_t* smark, int32_t lo_k,
-                                            bool valid, int32_t it, int32_t* rr, int32_t c, TileList& L,
-                                            long long* edge_acc) {
+                                            bool valid, int32_t it, int32_t b, int32_t e, int32_t c,
+                                            TileList& L, long long* edge_acc) {
     const int lane = threadIdx.x & 31;
-    int32_t dir = 0, b = 0, e = 0;
+    int32_t dir = 0;
     if (valid) {
         int32_t v = it & ITEM_MASK;
         dir = (it >> DIR_SHIFT) & 1;
-        if (rr[0] < 0) {
-            const int4* rp = rec_of(t, v, dir);
-            int4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
-            rr[0] = r0.x; rr[1] = r0.y; rr[2] = r0.z; rr[3] = r0.w; rr[4] = r1.x; rr[5] = r1.y; rr[6] = r1.z;
-            rr[7] = r1.w;
+        if (b < 0) {
+            const int32_t* off = dir ? a.r_begin : a.begin;
+            b = __ldg(off + v); e = __ldg(off + v + 1);
             c = __ldg(a.color + v);
         }
-        b = rr[0];
-        e = rr[1];
         *edge_acc += e - b;
+    } else {
+        b = e = 0;
     }
     int32_t deg = e - b;
     // long lists: the whole warp, 32 neighbours per step
@@ -259,42 +205,47 @@ __device__ __forceinline__ void tile_expand(const RoundArgs& a, const TileArgs& 
         int32_t lb = __shfl_sync(0xFFFFFFFFu, b, l), le = __shfl_sync(0xFFFFFFFFu, e, l);
         int32_t lc = __shfl_sync(0xFFFFFFFFu, c, l), ld = __shfl_sync(0xFFFFFFFFu, dir, l);
         const int32_t* adj = ld ? a.r_node_idx : a.node_idx;
+        const int32_t* off = ld ? a.r_begin : a.begin;
         for (int32_t k0 = lb; k0 < le; k0 += 32) {
             int32_t k = k0 + lane;
             int r = 0;
-            int32_t w = 0;
-            int4 r0 = make_int4(-1, -1, -1, -1), r1 = r0;
+            int32_t w = 0, wb = -1, we = -1;
             if (k < le) {
                 w = __ldg(adj + k);
-                r = tile_visit(a, t, smark, lo_k, w, ld, lc, r0, r1);
+                unsigned gm = *(volatile uint8_t*)(a.mark + w);
+                int32_t col = __ldg(a.color + w);
+                wb = __ldg(off + w); we = __ldg(off + w + 1);
+                if (col == lc) r = tile_claim(a, smark, lo_k, t.span, w, ld, gm);
             }
-            L.push(r == 1, w | (ld << DIR_SHIFT), r0, r1, lc);
+            L.push(r == 1, w | (ld << DIR_SHIFT), wb, we, lc);
             tile_send(a, t, r == 2, w | (ld << DIR_SHIFT));
         }
     }
-    // short lists: four neighbours per step, the first six from the record
+    // short lists: four neighbours per step, loads issued together
     int32_t mydeg = deg <= 32 ? deg : 0;
     int32_t maxd = (int32_t)__reduce_max_sync(0xFFFFFFFFu, (unsigned)mydeg);
     const int32_t* adj = dir ? a.r_node_idx : a.node_idx;
+    const int32_t* off = dir ? a.r_begin : a.begin;
     for (int32_t j0 = 0; j0 < maxd; j0 += 4) {
-        int32_t w[4];
+        int32_t w[4], col[4], wb[4], we[4];
+        unsigned gm[4];
         int r[4];
-        int4 q0[4], q1[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) w[u] = (j0 + u) < mydeg ? __ldg(adj + b + j0 + u) : -1;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            int32_t j = j0 + u;
-            int32_t inl = j == 0 ? rr[2] : j == 1 ? rr[3] : j == 2 ? rr[4] : j == 3 ? rr[5] : j == 4 ? rr[6] : rr[7];
-            w[u] = j < mydeg ? (j < REC_INLINE ? inl : __ldg(adj + b + j)) : -1;
+            bool p = w[u] >= 0;
+            gm[u] = p ? (unsigned)*(volatile uint8_t*)(a.mark + w[u]) : 0u;
+            col[u] = p ? __ldg(a.color + w[u]) : 0;
+            wb[u] = p ? __ldg(off + w[u]) : -1;
+            we[u] = p ? __ldg(off + w[u] + 1) : -1;
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            q0[u] = make_int4(-1, -1, -1, -1);
-            q1[u] = q0[u];
-            r[u] = w[u] >= 0 ? tile_visit(a, t, smark, lo_k, w[u], dir, c, q0[u], q1[u]) : 0;
-        }
+        for (int u = 0; u < 4; ++u)
+            r[u] = (w[u] >= 0 && col[u] == c) ? tile_claim(a, smark, lo_k, t.span, w[u], dir, gm[u]) : 0;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            L.push(r[u] == 1, w[u] | (dir << DIR_SHIFT), q0[u], q1[u], c);
+            L.push(r[u] == 1, w[u] | (dir << DIR_SHIFT), wb[u], we[u], c);
             tile_send(a, t, r[u] == 2, w[u] | (dir << DIR_SHIFT));
         }
     }
@@ -315,8 +266,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_reach_tile(RoundArgs a, Til
     int32_t* my_head = t.tctr + k * TILE_CTR_STRIDE;
     int32_t* my_tail = my_head + TILE_TAIL_OFF;
     int32_t* inbox = t.tq + (int64_t)k * t.inbox_cap;
-    TileList L{lists + wid * TILE_WBUF, lists + (TILE_WARPS + wid) * TILE_WBUF,
-               lists + 2 * TILE_WARPS * TILE_WBUF + wid * TILE_WBUF * 8, 0, 0, W, my_tail, inbox, t.inbox_cap, err};
+    TileList L{lists + (0 * TILE_WARPS + wid) * TILE_WBUF, lists + (1 * TILE_WARPS + wid) * TILE_WBUF,
+               lists + (2 * TILE_WARPS + wid) * TILE_WBUF, lists + (3 * TILE_WARPS + wid) * TILE_WBUF, 0, 0,
+               W, my_tail, inbox, t.inbox_cap, err, t.keep};
 
     // this tile's marks, two bits per vertex
     const int32_t words = t.span >> 4;
@@ -418,7 +370,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_reach_tile(RoundArgs a, Til
             L.pushed -= got - __popc(bal);          // dropped copies leave the count
             if (acc) {
                 int32_t pos = __popc(bal & ((1u << lane) - 1u));
-                L.it[pos] = (int32_t)((uint32_t)item & ~TILE_PRE); L.r[pos * 8] = -1; L.c[pos] = 0;
+                L.it[pos] = (int32_t)((uint32_t)item & ~TILE_PRE); L.b[pos] = -1; L.e[pos] = -1; L.c[pos] = 0;
             }
             __syncwarp();
             L.count = __popc(bal);
@@ -427,13 +379,12 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_reach_tile(RoundArgs a, Til
         int32_t kk = min(32, L.count);
         int32_t top = L.count - kk + lane;
         int32_t it = (lane < kk) ? L.it[top] : 0;
+        int32_t ib = (lane < kk) ? L.b[top] : 0;
+        int32_t ie = (lane < kk) ? L.e[top] : 0;
         int32_t ic = (lane < kk) ? L.c[top] : 0;
-        int32_t rr[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) rr[q] = (lane < kk) ? L.r[top * 8 + q] : 0;
         __syncwarp();
         L.count -= kk;
-        tile_expand(a, t, smark, lo_k, lane < kk, it, rr, ic, L, &my_edges);
+        tile_expand(a, t, smark, lo_k, lane < kk, it, ib, ie, ic, L, &my_edges);
         my_items += kk;
         L.pushed -= kk;
         if ((++iter & 7) == 0) {
@@ -449,7 +400,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 1) k_reach_tile(RoundArgs a, Til
             if (stop) { bailed = stop == 1; break; }
         }
         // share what this warp cannot expand in its next iteration
-        if (L.count > 2 * TILE_KEEP && !L.spill(TILE_KEEP)) break;
+        if (L.count > 2 * t.keep && !L.spill(t.keep)) break;
     }
     for (int o = 16; o > 0; o >>= 1) my_edges += __shfl_down_sync(0xFFFFFFFFu, my_edges, o);
     if (lane == 0) {
@@ -529,6 +480,7 @@ bool scc_impl_tile_eligible(const scc_state* s, int32_t live_lo, int32_t live_hi
 
 int scc_impl_reach_tile(const scc_graph* g, scc_state* s, RoundArgs& a, const int32_t* qin, int32_t qlen,
                         int32_t* qout, int32_t live_lo, int32_t live_hi, int32_t* handed_back) {
+    (void)g;
     *handed_back = 0;
     int blocks = tile_blocks(s->device);
     TileArgs t;
@@ -559,15 +511,7 @@ int scc_impl_reach_tile(const scc_graph* g, scc_state* s, RoundArgs& a, const in
     t.tctr = s->tctr;
     t.qout = qout;
     t.qcap = 2LL * s->n + 64;
-    // the graph's vertex records, built once per graph contents
-    if (!g->rec_valid) {
-        if (!g->rec) SCC_CUDA(cudaMalloc(&g->rec, sizeof(int4) * 4 * (size_t)std::max<int32_t>(g->n, 1)));
-        k_build_rec<<<scc_blocks(g->n, SCC_THREADS, 148 * 16), SCC_THREADS, 0, s->stream>>>(
-            g->n, g->begin, g->node_idx, g->r_begin, g->r_node_idx, g->rec);
-        SCC_LAUNCHED(s);
-        g->rec_valid = true;
-    }
-    t.rec = g->rec;
+    t.keep = std::min<int32_t>(std::max<int32_t>(s->tune.async_keep, 4), 64);
     SCC_CUDA(cudaMemsetAsync(s->tctr, 0, sizeof(int32_t) * TILE_CTR_WORDS, s->stream));
     SCC_CUDA(cudaMemcpyAsync(s->tctr + TILE_W, &qlen, sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
     SCC_TRY(scc_zero_counters(s, CTR_QLEN, 1));

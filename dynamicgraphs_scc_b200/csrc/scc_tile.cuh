@@ -4,8 +4,8 @@
 #include "scc_round.cuh"
 
 #define TILE_THREADS 512
-#define TILE_WBUF 192                 // per-warp list (items, each with its class and 32-byte record)
-#define TILE_KEEP 32                  // items a warp keeps when it shares the rest
+#define TILE_WBUF 256                 // per-warp list (items)
+
 #define TILE_MARK_WORDS 16384         // shared marks: 2 bits per vertex
 #define TILE_MAX_SPAN (TILE_MARK_WORDS * 16)
 #define TILE_MAX_TILES 160            // at least one per SM of a B200 (148)

@@ -357,7 +357,6 @@ extern "C" int scc_update_batch(scc_graph* g, scc_state* s, int64_t n_ins, const
     release_graph_arrays(g, st);
     g->begin = nb; g->node_idx = na; g->r_begin = nrb; g->r_node_idx = nra; g->m = m1;
     g->self_loops = -1;
-    g->rec_valid = false;
     g->async_arrays = true;
     SCC_CUDA(cudaEventRecord(s->ev[9], st));
 
@@ -471,7 +470,6 @@ extern "C" int scc_insert_idea1(scc_graph* g, scc_state* s, int64_t n_ins, const
     release_graph_arrays(g, st);
     g->begin = nb; g->node_idx = na; g->r_begin = nrb; g->r_node_idx = nra; g->m = m1;
     g->self_loops = -1;
-    g->rec_valid = false;
     g->async_arrays = true;
     SCC_TRY(scc_state_reset(s));
     return scc_run(g, s, SCC_METHOD_GLOBAL_WCC_FB, SCC_PIVOT_DEGREE, stats);
