@@ -234,6 +234,9 @@ def run_reference_cuda(args, workload):
     if os.path.exists(p):
         with open(p) as f:
             ref = json.load(f).get(workload, {})
+    if not ref and n <= (1 << 22):          # small workloads: the oracle's Tarjan directly
+        exp = O.tarjan_canonical(csr[0], csr[1])
+        ref = {"labels_sha256": hashlib.sha256(np.ascontiguousarray(exp, dtype="<i4").tobytes()).hexdigest()}
     return {"impl": "reference-cuda", "metric": "SCC GTEPS (edges / end-to-end decomposition time)",
             "value": round(m / (ms * 1e-3) / 1e9, 6), "unit": "GTEPS", "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms, 3), "higher_is_better": True, "dtype": "int32", "n_gpus": 1,

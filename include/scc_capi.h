@@ -175,13 +175,14 @@ typedef struct scc_tuning {
     int32_t async_blocks_per_sm;  /* resident blocks per SM in the drain (1, max 8) */
     int32_t huge_deg;             /* degree above which a top-down item is expanded edge-parallel (4096) */
     int32_t tile_min_live;        /* rounds with at least this many live vertices drain narrow frontiers
-                                     tile by tile (one id range per SM, marks in shared memory) (1 << 20);
-                                     negative = never */
+                                     tile by tile (one id range per SM, marks in shared memory); negative =
+                                     never (the default) */
     int32_t tile_min_span;        /* smallest id range of a tile (2048) */
     int32_t pivot_salt;           /* xor on vertex ids before the degree rule's tie-break hash (0): picks
                                      another of the equally good pivots; changes speed, never labels */
     int32_t tail_live;            /* from the second recursion round on, at most this many live vertices are
-                                     finished in one launch, a block per class (1 << 20); negative = never */
+                                     finished in one launch, a block per class; negative = never (the
+                                     default) */
     int32_t tail_class;           /* ... provided no class has more vertices than this (1 << 16) */
 } scc_tuning;
 int scc_state_get_tuning(scc_state* s, scc_tuning* t);
