@@ -298,6 +298,11 @@ def bench_batched(args, local_rank):
     ms = statistics.mean(r["ms_total"] for r in runs)
     labels = st.canonical_labels()
     plan.free()
+    if args.batch_only:
+        print(json.dumps({"metric": "SCC GTEPS, batched uneven graphs (one persistent launch from a CUDA graph)",
+                          "value": round(m / (ms * 1e-3) / 1e9, 4), "unit": "GTEPS", "ms_per_step": round(ms, 3),
+                          "config": {"graphs": args.batch_graphs, "n": n, "m": m, "autotuned": best}}))
+        return
     # the general engine over the disjoint union (many kernel launches, host-driven rounds)
     st.reset(); st.run(2)
     union_runs = []
@@ -709,6 +714,7 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c4", "c5", "levels"])
     ap.add_argument("--tune-trials", type=int, default=8)
     ap.add_argument("--batch-graphs", type=int, default=4096, help="c4: graphs in the batch")
+    ap.add_argument("--batch-only", action="store_true", help="c4: skip the union-engine and per-graph comparisons")
     ap.add_argument("--batches", type=int, default=10000, help="c5: batches at the configured arrival rate")
     ap.add_argument("--sustain-batches", type=int, default=2000,
                     help="c5: batches at a rate the service sustains (0 = skip)")
