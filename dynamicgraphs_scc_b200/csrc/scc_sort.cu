@@ -13,10 +13,12 @@
 //  2. an exclusive scan of those counts gives every (digit, tile) its first
 //     output position;
 //  3. k_rs_scatter: each tile walks its 16 rounds in order; inside a round an
-//     element's position is its digit's running position plus the elements of
-//     that digit in earlier warps (per-warp counts in shared memory) plus the
-//     earlier lanes of its warp with that digit (__match_any_sync).  Elements
-//     leave in input order within each digit, so the sort is stable.
+//     element's slot is its digit's running slot plus the elements of that
+//     digit in earlier warps (per-warp counts in shared memory) plus the
+//     earlier lanes of its warp with that digit (__match_any_sync).  The tile
+//     is reordered by digit in shared memory first, then written out run by
+//     run, so the writes are coalesced.  Elements keep their input order
+//     within each digit, so the sort is stable.
 #include "scc_internal.cuh"
 #include "scc_sort.cuh"
 
@@ -129,19 +131,36 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__
                                                            const int32_t* __restrict__ vin,
                                                            int32_t* __restrict__ vout, int64_t m, int shift,
                                                            int32_t ntiles, const int32_t* __restrict__ offs) {
-    __shared__ int32_t run[RS_BINS];
+    __shared__ int32_t run[RS_BINS];              // next tile-local slot of each digit
+    __shared__ int32_t start[RS_BINS];            // tile-local start of each digit
     __shared__ int32_t wcnt[RS_WARPS][RS_BINS];
+    __shared__ K skey[RS_TILE];
+    __shared__ int32_t sval[VALS ? RS_TILE : 1];
+    __shared__ int32_t s_w[RS_WARPS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int j = threadIdx.x; j < RS_WARPS * RS_BINS; j += RS_THREADS) (&wcnt[0][0])[j] = 0;
     for (int32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        run[threadIdx.x] = offs[(int64_t)threadIdx.x * ntiles + tile];
+        const int64_t base = (int64_t)tile * RS_TILE;
+        const int32_t cnt = (m - base < RS_TILE) ? (int32_t)(m - base) : RS_TILE;
+        // the tile's own histogram, and each digit's start inside the tile
+        run[threadIdx.x] = 0;
         __syncthreads();
-        int64_t base = (int64_t)tile * RS_TILE;
         for (int r = 0; r < RS_ITEMS; ++r) {
-            int64_t i = base + r * RS_THREADS + threadIdx.x;
-            bool valid = i < m;
-            K k = valid ? kin[i] : (K)0;
-            int32_t v = (VALS && valid) ? vin[i] : 0;
+            int32_t j = r * RS_THREADS + threadIdx.x;
+            if (j < cnt) atomicAdd(&run[(unsigned)(kin[base + j] >> shift) & (RS_BINS - 1)], 1);
+        }
+        __syncthreads();
+        int32_t tot = 0;
+        int32_t st0 = block_excl256(run[threadIdx.x], s_w, &tot);
+        start[threadIdx.x] = st0;
+        run[threadIdx.x] = st0;
+        __syncthreads();
+        // stable ranks: rounds in input order, warps in order, lanes in order
+        for (int r = 0; r < RS_ITEMS; ++r) {
+            int32_t j = r * RS_THREADS + threadIdx.x;
+            bool valid = j < cnt;
+            K k = valid ? kin[base + j] : (K)0;
+            int32_t v = (VALS && valid) ? vin[base + j] : 0;
             int d = valid ? (int)((unsigned)(k >> shift) & (RS_BINS - 1)) : RS_BINS + lane;   // invalid lanes match nobody
             unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
             int lr = __popc(peers & ((1u << lane) - 1u));
@@ -151,9 +170,9 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__
             if (valid) {
                 int32_t pre = 0;
                 for (int w = 0; w < wid; ++w) pre += wcnt[w][d];
-                int64_t pos = (int64_t)run[d] + pre + lr;
-                kout[pos] = k;
-                if (VALS) vout[pos] = v;
+                int32_t pos = run[d] + pre + lr;
+                skey[pos] = k;
+                if (VALS) sval[pos] = v;
             }
             __syncthreads();
             if (valid && leader) {
@@ -162,6 +181,16 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__
             }
             __syncthreads();
         }
+        // the tile leaves in digit order: consecutive threads write consecutive
+        // slots of each digit's run
+        for (int32_t j = threadIdx.x; j < cnt; j += RS_THREADS) {
+            K k = skey[j];
+            int d = (int)((unsigned)(k >> shift) & (RS_BINS - 1));
+            int64_t pos = (int64_t)offs[(int64_t)d * ntiles + tile] + (j - start[d]);
+            kout[pos] = k;
+            if (VALS) vout[pos] = sval[j];
+        }
+        __syncthreads();
     }
 }
 
@@ -221,10 +250,14 @@ static int radix_sort(const K* keys_in, K* keys_out, const int32_t* vals_in, int
             e = cudaPeekAtLastError();
             if (e == cudaSuccess) e = scan_excl(cnt, L, sums, st);
             if (e != cudaSuccess) break;
-            if (vals)
-                k_rs_scatter<K, true><<<blocks, RS_THREADS, 0, st>>>(ksrc, kbuf[cur], vsrc, vbuf[cur], m, shift,
-                                                                    ntiles, cnt);
-            else
+            if constexpr (sizeof(K) == 4) {      // values ride along with 32-bit keys only
+                if (vals)
+                    k_rs_scatter<K, true><<<blocks, RS_THREADS, 0, st>>>(ksrc, kbuf[cur], vsrc, vbuf[cur], m, shift,
+                                                                        ntiles, cnt);
+                else
+                    k_rs_scatter<K, false><<<blocks, RS_THREADS, 0, st>>>(ksrc, kbuf[cur], nullptr, nullptr, m,
+                                                                         shift, ntiles, cnt);
+            } else
                 k_rs_scatter<K, false><<<blocks, RS_THREADS, 0, st>>>(ksrc, kbuf[cur], nullptr, nullptr, m, shift,
                                                                      ntiles, cnt);
             e = cudaPeekAtLastError();
