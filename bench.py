@@ -42,6 +42,9 @@ WORKLOADS = {
     # smaller cases of the same shapes, for profiler captures
     "rmat22": dict(rmat_scale=22, edge_factor=16, seed=2024),
     "grid4096": dict(grid_side=4096, seed=2024),
+    # mid-degree hubs: top-down levels full of items between one warp's and the
+    # edge-parallel path's degrees (the block-wide expansion's workload)
+    "hubs": dict(hubs_n=1 << 22, hubs=30000, hub_deg=(64, 4000), seed=5),
 }
 # CPU-baseline sample of the same workload shape at 1/16 of the vertices
 CPU_SAMPLES = {
@@ -51,6 +54,7 @@ CPU_SAMPLES = {
     "c1": dict(rmat_scale=16, edge_factor=8, seed=42),
     "rmat22": dict(rmat_scale=18, edge_factor=16, seed=2024),
     "grid4096": dict(grid_side=1024, seed=2024),
+    "hubs": dict(hubs_n=1 << 18, hubs=1875, hub_deg=(64, 4000), seed=5),
 }
 WORKLOAD_NAMES = {
     "c2": "R-MAT s24 ef16 (a=.57,b=.19,c=.19) U 4096x4096 randomly oriented grid (+5% bidirectional)",
@@ -59,6 +63,7 @@ WORKLOAD_NAMES = {
     "c1": "R-MAT s16 ef8 (a=.57,b=.19,c=.19)",
     "rmat22": "R-MAT s22 ef16 (a=.57,b=.19,c=.19)",
     "grid4096": "4096x4096 randomly oriented grid (+5% bidirectional)",
+    "hubs": "4M-vertex random digraph (out-degree 2) + 30,000 hubs of extra out- and in-degree uniform [64, 4000)",
 }
 
 
@@ -147,14 +152,43 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(sm)}
 
 
+def hub_edges(hubs_n, hubs, hub_deg, seed):
+    """A random digraph of out-degree 2 on hubs_n vertices plus `hubs` distinct
+    vertices with extra out- and in-edges, degrees uniform in hub_deg."""
+    rng = np.random.default_rng(seed)
+    s = [np.repeat(np.arange(hubs_n, dtype=np.int32), 2)]
+    d = [rng.integers(0, hubs_n, 2 * hubs_n, dtype=np.int32)]
+    for h in rng.choice(hubs_n, hubs, replace=False):
+        k_out, k_in = rng.integers(hub_deg[0], hub_deg[1], 2)
+        s += [np.full(k_out, h, np.int32), rng.integers(0, hubs_n, k_in, dtype=np.int32)]
+        d += [rng.integers(0, hubs_n, k_out, dtype=np.int32), np.full(k_in, h, np.int32)]
+    return hubs_n, np.concatenate(s), np.concatenate(d)
+
+
+def workload_edges(kw):
+    """Seeded edge list (n, src, dst) of a workload, on the host."""
+    from dynamicgraphs_scc_b200 import generate_edges_host
+    if "hubs" in kw:
+        return hub_edges(**kw)
+    return generate_edges_host(**kw)
+
+
+def workload_graph(kw, device):
+    """The workload's graph on the device (generated there where it can be)."""
+    from dynamicgraphs_scc_b200 import Graph
+    if "hubs" in kw:
+        n, s, d = hub_edges(**kw)
+        return Graph.from_edges(n, s, d, device=device)
+    return Graph.generate(**kw, device=device)
+
+
 def host_csr(kw):
     """Seeded edge list of a workload -> forward CSR on the host (self-loops and
     duplicates removed; the oracle's dedup leaves the edges sorted by (source,
     target), so the CSR is its offsets and targets).  Input preparation for the
     reference's own engine, which builds its reverse edges itself."""
     from oracle import oracle as O
-    from dynamicgraphs_scc_b200 import generate_edges_host
-    n, s, d = generate_edges_host(**kw)
+    n, s, d = workload_edges(kw)
     s, d = O.dedup_edges(s, d, n=n)
     b = np.zeros(n + 1, np.int32)
     np.cumsum(np.bincount(s, minlength=n), out=b[1:])
@@ -214,7 +248,7 @@ def run_reference_cuda(args, workload):
     if not O.ref_cuda_available():
         return {"impl": "reference-cuda", "unavailable": "the reference's CUDA engine was not built (oracle/Makefile)"}
     kw = WORKLOADS[workload]
-    n, s, d = generate_edges_host(**kw)
+    n, s, d = workload_edges(kw)
     s, d = O.dedup_edges(s, d, n=n)
     csr = O.build_csr(n, s, d)
     m = int(csr[1].size)
@@ -361,6 +395,9 @@ def _pct(xs, p):
     return xs[min(len(xs) - 1, int(p * (len(xs) - 1) + 0.5))] if xs else None
 
 
+SUSTAIN_HEADROOM = 3.0
+
+
 def bench_serving(args, local_rank, batches_n=None, sustain_n=None):
     """Streaming updates against a device-resident R-MAT s22 ef16 graph through the
     serving loop: batches arrive Poisson (mean 2 ms), sizes log-uniform in
@@ -374,9 +411,13 @@ def bench_serving(args, local_rank, batches_n=None, sustain_n=None):
     backlog limit in edges, and an age limit) so the queue stays bounded;
     offered, served and shed load are reported.  "sustainable": after the
     queue has drained, the same batch distribution at a mean gap the service
-    sustains (1.5 x the mean service time of the configured phase's last 100
-    admitted batches), where p50/p99 describe the system rather than the
-    length of the run.  Returns the JSON line."""
+    sustains (SUSTAIN_HEADROOM x the mean service time of the configured
+    phase's last 100 admitted batches: the device busy about a third of the
+    time, since the service time is heavy-tailed and queueing delay grows with
+    its second moment), where p50/p99 describe the system rather than the
+    length of the run.  A check waits for the batches before it and copies the
+    graph out; the arrival clock stops meanwhile (rates and wall times leave
+    the pauses out).  Returns the JSON line."""
     import multiprocessing as mp
     from concurrent.futures import ProcessPoolExecutor
     import torch
@@ -427,12 +468,16 @@ def bench_serving(args, local_rank, batches_n=None, sustain_n=None):
             else:
                 pending.append((rid, edges))
             counter["batches"] += 1
-            t_last = time.perf_counter()
             if counter["batches"] % 100 == 0:
+                # the check needs the session idle at this batch; the arrival
+                # clock stops meanwhile, so no burst of late arrivals follows it
+                tp = time.perf_counter()
                 results += [(sv.wait(r), e) for r, e in pending]
                 pending = []
                 cb, ca, _, _ = sv.session_csr(sid)
                 checks.append(pool.submit(_tarjan_equal, cb, ca, sv.labels(sid)))
+                t0 += time.perf_counter() - tp
+            t_last = time.perf_counter()
         arrival_s = max(t_last - t0, 1e-9)
         results += [(sv.wait(r), e) for r, e in pending]
         wall = time.perf_counter() - t0
@@ -459,8 +504,8 @@ def bench_serving(args, local_rank, batches_n=None, sustain_n=None):
     configured = run_phase(batches_n, 2.0)
     sv.drain()                  # the second phase starts from an empty queue
     # the service time grows with the graph (inserts outnumber deletes), so the
-    # sustainable gap follows the latest admitted batches, with 50 % headroom
-    gap = 1.5 * (configured["service_ms"]["mean_last_100"] or 2.0)
+    # sustainable gap follows the latest admitted batches
+    gap = SUSTAIN_HEADROOM * (configured["service_ms"]["mean_last_100"] or 2.0)
     sustainable = run_phase(sustain_n, gap) if sustain_n > 0 else None
     sv.drain()
     st = sv.stats()
@@ -805,7 +850,7 @@ def main():
     kw = WORKLOADS[args.workload]
     learned = args.workload == "c3"            # the learned-pivot configuration
     model, model_info = (train_pivot_model(local_rank) if learned else (None, None))
-    g = Graph.generate(**kw, device=local_rank)
+    g = workload_graph(kw, local_rank)
     n, m = g.num_nodes(), g.num_edges()
     st = State(g)
     if model is not None:

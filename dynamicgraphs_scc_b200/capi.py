@@ -76,7 +76,7 @@ class ServerStats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [(k, C.c_int32) for k in ("bu_alpha", "bu_div", "async_max", "async_after", "async_keep",
                                          "async_blocks_per_sm", "huge_deg", "tile_min_live", "tile_min_span",
-                                         "pivot_salt", "tail_live", "tail_class")]
+                                         "pivot_salt", "tail_live", "tail_class", "cta_deg")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -188,6 +188,8 @@ static RoundArgs round_args(const scc_graph* g, scc_state* s) {
     a.async_keep = s->tune.async_keep;
     a.async_bail = std::max<int32_t>(8 * s->tune.async_max, 1 << 16);
     a.pivot_salt = (uint32_t)s->tune.pivot_salt;
+    a.cta_deg = s->tune.cta_deg;
+    round_args_adjacency(a, g->node_idx, g->r_node_idx, g->m);
     return a;
 }
 

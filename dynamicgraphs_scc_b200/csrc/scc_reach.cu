@@ -8,13 +8,18 @@
 // Three execution modes, chosen per step by the host from the frontier size:
 //
 //  * top-down level (k_reach_level): one launch per BFS level; a warp takes 32
-//    items, vertices with more than 32 neighbours are expanded by the whole
-//    warp (coalesced adjacency reads), the rest lane by lane; new items go to
-//    a per-warp shared-memory buffer and reach the global queue in batches;
+//    items; vertices above huge_deg neighbours go edge-parallel over the
+//    grid (k_reach_huge), those above cta_deg are expanded by the whole block
+//    with their adjacency streamed into shared memory by bulk copies, those
+//    above 32 by the whole warp (coalesced adjacency reads), the rest lane by
+//    lane; new items go to a per-warp shared-memory buffer and reach the
+//    global queue in batches;
 //  * bottom-up sweep (k_reach_bottomup): when the frontier is a large share of
 //    the live vertices (the "RD" state of gm_bfs_template.h:418-487), every
 //    unvisited live vertex looks for an already visited parent among its
-//    in-neighbours (FW) / out-neighbours (BW) and stops at the first one;
+//    in-neighbours (FW) and a visited child among its out-neighbours (BW),
+//    both searches in step, int4 chunks of adjacency at a time, and stops
+//    each at its first hit;
 //  * asynchronous drain (k_reach_async): once the frontier has stayed narrow
 //    for a few levels (long-diameter inputs such as grids and long cycles),
 //    one persistent launch finishes the traversal with no level barriers and
@@ -45,7 +50,8 @@
 template <class Push>
 __device__ __forceinline__ void expand_warp(const RoundArgs& a, bool valid, int32_t it, Push& push,
                                             int32_t* huge_list = nullptr, int32_t* huge_cnt = nullptr,
-                                            long long* edge_acc = nullptr) {
+                                            long long* edge_acc = nullptr, int32_t* cta_list = nullptr,
+                                            int32_t* cta_cnt = nullptr) {
     int lane = threadIdx.x & 31;
     int32_t v = 0, dir = 0, b = 0, e = 0, c = 0;
     if (valid) {
@@ -58,6 +64,9 @@ __device__ __forceinline__ void expand_warp(const RoundArgs& a, bool valid, int3
         if (edge_acc) *edge_acc += e - b;
         if (huge_list && e - b > a.huge_deg) {
             huge_list[atomicAdd(huge_cnt, 1)] = it;
+            e = b;
+        } else if (cta_list && e - b > a.cta_deg) {
+            cta_list[atomicAdd(cta_cnt, 1)] = it;      // the block expands it (expand_block)
             e = b;
         }
     }
@@ -158,19 +167,148 @@ struct GlobalPush {
     }
 };
 
+// ------------------------------------------------------------------ block-wide expansion
+// A top-down item of degree in (cta_deg, huge_deg] is expanded by the whole
+// block: its adjacency list is streamed into shared memory in chunks of
+// CTA_STAGE entries by 1-D bulk copies (cp.async.bulk, global memory of this
+// GPU into this CTA's shared memory, completion counted on an mbarrier), two
+// buffers deep, so the next chunk is in flight while the block visits the
+// current one.  A copy starts and ends on 16-byte boundaries: the staged
+// range is [b & ~3, e & ~3) (entries before b are masked) and the last
+// (e & 3) entries are read directly.
+#define CTA_STAGE 1024
+#define BULK_WAIT_LIMIT (1 << 20)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Copy `bytes` (a multiple of 16, both addresses 16-byte aligned) from global
+// memory into shared memory; the copy's bytes complete the barrier's phase.
+__device__ __forceinline__ void bulk_stage(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait for the barrier's phase of the given parity.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity) {
+    for (int i = 0; i < BULK_WAIT_LIMIT; ++i) {
+        uint32_t ok;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+struct BlockStage {
+    int32_t buf[2][CTA_STAGE];
+    unsigned long long bar[2];
+    int32_t list[REACH_THREADS];     // items deferred to the block in this pass
+    int32_t count;
+};
+
+// Expand [b, e) (direction dir, class c) with every thread of the block.
+// Block-uniform; returns false (error word set) if a copy did not complete
+// within its bound, after waiting once more, bounded, for copies in flight.
+template <class Push>
+__device__ bool expand_block(const RoundArgs& a, int32_t b, int32_t e, int32_t c, int32_t dir, BlockStage& st,
+                             uint32_t& parity, Push& push) {
+    const int32_t* adj = dir ? a.r_node_idx : a.node_idx;
+    const int tid = threadIdx.x;
+    const int32_t lo = b & ~3, hi = e & ~3;
+    const int32_t nchunks = (a.vec_adj && hi > lo) ? (hi - lo + CTA_STAGE - 1) / CTA_STAGE : 0;
+    if (nchunks > 0 && tid == 0)
+        bulk_stage(st.buf[0], adj + lo, 4u * (uint32_t)min(CTA_STAGE, hi - lo), &st.bar[0]);
+    for (int32_t t = 0; t < nchunks; ++t) {
+        const int32_t x0 = lo + t * CTA_STAGE, x1 = min(hi, x0 + CTA_STAGE);
+        const int nb = (t + 1) & 1;
+        if (t + 1 < nchunks && tid == 0)   // buffer nb was released by the barrier that ended chunk t - 1
+            bulk_stage(st.buf[nb], adj + x1, 4u * (uint32_t)(min(hi, x1 + CTA_STAGE) - x1), &st.bar[nb]);
+        const int cb = t & 1;
+        const uint32_t ph = (parity >> cb) & 1u;
+        bool ok = mbar_wait(&st.bar[cb], ph);
+        parity ^= 1u << cb;
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicExch(a.ctr + CTR_ERROR, SCC_DEVERR_WAIT_LIMIT);
+                atomicExch(a.ctr + CTR_ERROR_INFO, 3);
+            }
+            if (!ok) mbar_wait(&st.bar[cb], ph);
+            if (t + 1 < nchunks) mbar_wait(&st.bar[nb], (parity >> nb) & 1u);
+            return false;
+        }
+        for (int32_t k0 = max(b, x0); k0 < x1; k0 += REACH_THREADS) {
+            const int32_t k = k0 + tid;
+            bool p = false;
+            int32_t w = 0;
+            if (k < x1) { w = st.buf[cb][k - x0]; p = visit(a, w, c, dir); }
+            push(p, w | (dir << DIR_SHIFT));
+        }
+        __syncthreads();
+    }
+    for (int32_t k0 = nchunks > 0 ? max(b, hi) : b; k0 < e; k0 += REACH_THREADS) {
+        const int32_t k = k0 + tid;
+        bool p = false;
+        int32_t w = 0;
+        if (k < e) { w = __ldg(adj + k); p = visit(a, w, c, dir); }
+        push(p, w | (dir << DIR_SHIFT));
+    }
+    return true;
+}
+
+// One top-down level.  BLOCK: items of degree in (cta_deg, huge_deg] are
+// collected per pass of REACH_THREADS items and expanded by the whole block
+// after the pass's warp and lane expansions.
+template <bool BLOCK>
 __global__ void __launch_bounds__(REACH_THREADS) k_reach_level(RoundArgs a, const int32_t* __restrict__ qin,
                                                                 int32_t nin, int32_t* __restrict__ qout,
                                                                 int32_t* __restrict__ huge_list) {
     __shared__ int32_t sbuf[REACH_THREADS / 32][WBUF];
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     GlobalPush push{sbuf[wid], 0, qout, a.ctr + CTR_QLEN, a.begin, a.r_begin, 0ull};
-    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    int64_t groups = ((int64_t)nin + 31) >> 5;
-    for (int64_t gi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; gi < groups; gi += nwarps) {
-        int64_t idx = gi * 32 + lane;
-        bool valid = idx < nin;
-        int32_t it = valid ? qin[idx] : 0;
-        expand_warp(a, valid, it, push, huge_list, a.ctr + CTR_SPARE4);
+    if constexpr (!BLOCK) {
+        int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+        int64_t groups = ((int64_t)nin + 31) >> 5;
+        for (int64_t gi = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; gi < groups; gi += nwarps) {
+            int64_t idx = gi * 32 + lane;
+            bool valid = idx < nin;
+            int32_t it = valid ? qin[idx] : 0;
+            expand_warp(a, valid, it, push, huge_list, a.ctr + CTR_SPARE4);
+        }
+    } else {
+        __shared__ __align__(16) BlockStage st;
+        if (threadIdx.x == 0) {
+            mbar_init(&st.bar[0], 1);
+            mbar_init(&st.bar[1], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            st.count = 0;
+        }
+        __syncthreads();
+        uint32_t parity = 0;
+        bool ok = true;
+        for (int64_t base = (int64_t)blockIdx.x * REACH_THREADS; base < nin && ok;
+             base += (int64_t)gridDim.x * REACH_THREADS) {
+            int64_t idx = base + threadIdx.x;
+            bool valid = idx < nin;
+            int32_t it = valid ? qin[idx] : 0;
+            expand_warp(a, valid, it, push, huge_list, a.ctr + CTR_SPARE4, nullptr, st.list, &st.count);
+            __syncthreads();
+            const int32_t nc = st.count;
+            for (int32_t j = 0; j < nc && ok; ++j) {
+                const int32_t ci = st.list[j], v = ci & ITEM_MASK, d = (ci >> DIR_SHIFT) & 1;
+                const int32_t* off = d ? a.r_begin : a.begin;
+                ok = expand_block(a, __ldg(off + v), __ldg(off + v + 1), __ldg(a.color + v), d, st, parity, push);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) st.count = 0;
+            __syncthreads();
+        }
     }
     push.finish(reinterpret_cast<unsigned long long*>(a.ctr + CTR_EDGES));
 }
@@ -236,39 +374,42 @@ __global__ void __launch_bounds__(REACH_THREADS) k_reach_huge(RoundArgs a, const
 }
 
 // ------------------------------------------------------------------ bottom-up mode
-// True if a neighbour of v carries `bit` in its mark and belongs to v's class.
-// Four neighbours at a time: their adjacency entries, then their marks, are
-// loaded together, so a long scan costs two round trips per four.  A round
-// over one class (use_only) traverses only that class, so a marked neighbour
-// is of colour c and its colour need not be read; with several classes a
-// mark may come from another class's traversal.
-__device__ __forceinline__ bool parent_ok(const RoundArgs& a, int32_t u, int32_t c) {
-    return a.use_only || __ldg(a.color + u) == c;
+// A round over one class (use_only) traverses only that class, so a marked
+// neighbour is of colour c and its colour need not be read; with several
+// classes a mark may come from another class's traversal.
+// Entries [k, e) of one adjacency list seen through the aligned chunk
+// [k & ~3, (k & ~3) + P): P/4 int4 loads (a 32-byte sector for P = 8) when
+// the chunk lies inside the array and the array is 16-byte aligned, else one
+// load per entry that lies in [k, e).  Entries outside [k, e) are masked.
+template <int P>
+__device__ __forceinline__ void probe_chunk(const RoundArgs& a, const int32_t* __restrict__ adj, int32_t k,
+                                            int32_t e, int32_t (&u)[P], bool (&p)[P]) {
+    const int32_t c0 = k & ~3;
+#pragma unroll
+    for (int j = 0; j < P; ++j) p[j] = k < e && c0 + j >= k && c0 + j < e;
+    if (k < e && a.vec_adj && (int64_t)c0 + P <= a.adj_len) {
+#pragma unroll
+        for (int q = 0; q < P / 4; ++q) {
+            int4 x = __ldg(reinterpret_cast<const int4*>(adj + c0) + q);
+            u[4 * q] = x.x; u[4 * q + 1] = x.y; u[4 * q + 2] = x.z; u[4 * q + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < P; ++j) u[j] = p[j] ? __ldg(adj + c0 + j) : 0;
+    }
 }
 
-__device__ __forceinline__ bool has_marked_parent(const RoundArgs& a, const int32_t* __restrict__ off,
-                                                  const int32_t* __restrict__ adj, int32_t v, int32_t c,
-                                                  unsigned bit) {
-    int32_t b = __ldg(off + v), e = __ldg(off + v + 1);
-    int32_t k = b;
-    for (; k + 4 <= e; k += 4) {
-        int32_t u[4];
-        unsigned m[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) u[j] = __ldg(adj + k + j);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) m[j] = *(volatile uint8_t*)(a.mark + u[j]);
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if ((m[j] & bit) && parent_ok(a, u[j], c)) return true;
-    }
-    for (; k < e; ++k) {
-        int32_t u = __ldg(adj + k);
-        if ((*(volatile uint8_t*)(a.mark + u) & bit) && parent_ok(a, u, c)) return true;
-    }
-    return false;
-}
-
+// One thread per live vertex, both directions at once: the vertex's colour,
+// mark and both adjacency ranges are loaded together, then each probe loads
+// an aligned chunk of each still-open list, then the marks of both chunks'
+// neighbours, then (in a round over several classes) the colours of the
+// marked ones -- three dependent round trips per probe for the two searches
+// together, where searching one direction after the other costs six.
+// P = 4 (one int4 per list and probe, 40 registers): R-MAT s24 1.274 ->
+// 1.243 ms and C3 2.29 -> 2.17 ms a decomposition against one direction
+// after the other; P = 8 (a whole 32-byte sector per probe) needs 64
+// registers, halves the resident warps and is slower on both (1.38, 2.48 ms).
+template <int P>
 __global__ void __launch_bounds__(REACH_THREADS) k_reach_bottomup(RoundArgs a, int32_t* __restrict__ qout) {
     __shared__ int32_t sbuf[REACH_THREADS / 32][WBUF];
     int wid = threadIdx.x >> 5;
@@ -281,18 +422,50 @@ __global__ void __launch_bounds__(REACH_THREADS) k_reach_bottomup(RoundArgs a, i
         if (i < a.live_count) {
             v = a.live[i];
             int32_t c = __ldg(a.color + v);
-            if (c != SCC_COLOR_DONE && (!a.use_only || c == a.only_color)) {
-                unsigned m = *(volatile uint8_t*)(a.mark + v);
-                if (!(m & 1u)) p0 = has_marked_parent(a, a.r_begin, a.r_node_idx, v, c, 1u);
-                if (!(m & 2u)) p1 = has_marked_parent(a, a.begin, a.node_idx, v, c, 2u);
-                if (p0 || p1) {
-                    unsigned sh = (unsigned)(v & 3) * 8u;
-                    unsigned bits = (p0 ? 1u : 0u) | (p1 ? 2u : 0u);
-                    unsigned old = atomicOr(reinterpret_cast<unsigned*>(a.mark + (v & ~3)), bits << sh);
-                    // push only directions this thread newly set
-                    p0 = p0 && !((old >> sh) & 1u);
-                    p1 = p1 && !((old >> sh) & 2u);
+            unsigned m = *(volatile uint8_t*)(a.mark + v);
+            int32_t k0 = __ldg(a.r_begin + v), e0 = __ldg(a.r_begin + v + 1);   // FW: a marked in-neighbour
+            int32_t k1 = __ldg(a.begin + v), e1 = __ldg(a.begin + v + 1);       // BW: a marked out-neighbour
+            bool in = c != SCC_COLOR_DONE && (!a.use_only || c == a.only_color);
+            if (!in || (m & 1u)) e0 = k0;
+            if (!in || (m & 2u)) e1 = k1;
+            while (k0 < e0 || k1 < e1) {
+                int32_t u0[P], u1[P];
+                bool q0[P], q1[P];
+                probe_chunk<P>(a, a.r_node_idx, k0, e0, u0, q0);
+                probe_chunk<P>(a, a.node_idx, k1, e1, u1, q1);
+                unsigned m0[P], m1[P];
+#pragma unroll
+                for (int j = 0; j < P; ++j) m0[j] = q0[j] ? (unsigned)*(volatile uint8_t*)(a.mark + u0[j]) : 0u;
+#pragma unroll
+                for (int j = 0; j < P; ++j) m1[j] = q1[j] ? (unsigned)*(volatile uint8_t*)(a.mark + u1[j]) : 0u;
+#pragma unroll
+                for (int j = 0; j < P; ++j) {
+                    q0[j] = q0[j] && (m0[j] & 1u);
+                    q1[j] = q1[j] && (m1[j] & 2u);
                 }
+                if (!a.use_only) {
+                    // a mark may come from another class's traversal
+#pragma unroll
+                    for (int j = 0; j < P; ++j) {
+                        int32_t c0 = q0[j] ? __ldg(a.color + u0[j]) : c;
+                        int32_t c1 = q1[j] ? __ldg(a.color + u1[j]) : c;
+                        q0[j] = q0[j] && c0 == c;
+                        q1[j] = q1[j] && c1 == c;
+                    }
+                }
+                bool h0 = false, h1 = false;
+#pragma unroll
+                for (int j = 0; j < P; ++j) { h0 = h0 || q0[j]; h1 = h1 || q1[j]; }
+                if (h0) { p0 = true; e0 = k0; } else { k0 = (k0 & ~3) + P; }
+                if (h1) { p1 = true; e1 = k1; } else { k1 = (k1 & ~3) + P; }
+            }
+            if (p0 || p1) {
+                unsigned sh = (unsigned)(v & 3) * 8u;
+                unsigned bits = (p0 ? 1u : 0u) | (p1 ? 2u : 0u);
+                unsigned old = atomicOr(reinterpret_cast<unsigned*>(a.mark + (v & ~3)), bits << sh);
+                // push only directions this thread newly set
+                p0 = p0 && !((old >> sh) & 1u);
+                p1 = p1 && !((old >> sh) & 2u);
             }
         }
         push(p0, v);
@@ -635,7 +808,8 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
         bool synced = false;      // the counters on the host already hold this step's results
         if (bottom_up) {
             SCC_TRY(scc_zero_counters(s, CTR_QLEN, 1));
-            k_reach_bottomup<<<scc_blocks(a.live_count, REACH_THREADS, 148 * 16), REACH_THREADS, 0, s->stream>>>(a, qout);
+            k_reach_bottomup<4><<<scc_blocks(a.live_count, REACH_THREADS, 148 * 16), REACH_THREADS, 0, s->stream>>>(
+                a, qout);
             SCC_LAUNCHED(s);
             narrow = 0;
             mode = "bottom-up";
@@ -720,10 +894,15 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
             SCC_TRY(scc_zero_counters(s, CTR_QLEN, 1));
             SCC_TRY(scc_zero_counters(s, CTR_SPARE4, 1));
             SCC_TRY(scc_zero_counters(s, CTR_EDGES, 2));
-            k_reach_level<<<scc_blocks((int64_t)qlen, REACH_THREADS, 148 * 8), REACH_THREADS, 0, s->stream>>>(
-                a, qin, qlen, qout, s->hq);
+            if (a.cta_deg > 0 && a.cta_deg < a.huge_deg)
+                k_reach_level<true><<<scc_blocks((int64_t)qlen, REACH_THREADS, 148 * 8), REACH_THREADS, 0, s->stream>>>(
+                    a, qin, qlen, qout, s->hq);
+            else
+                k_reach_level<false><<<scc_blocks((int64_t)qlen, REACH_THREADS, 148 * 8), REACH_THREADS, 0, s->stream>>>(
+                    a, qin, qlen, qout, s->hq);
             SCC_LAUNCHED(s);
             SCC_TRY(scc_sync_counters(s));
+            if (s->h_ctr[CTR_ERROR]) return scc_check_device_error(s);
             int32_t nhuge = s->h_ctr[CTR_SPARE4];
             if (nhuge > 0) {
                 k_huge_prefix<<<1, 1024, 0, s->stream>>>(a, s->hq, nhuge, s->hoff);

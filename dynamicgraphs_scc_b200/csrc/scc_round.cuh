@@ -21,7 +21,18 @@ struct RoundArgs {
     int32_t async_keep;         // items a warp keeps before sharing in the asynchronous drain
     int32_t async_bail;         // outstanding items at which the drain hands back to level steps
     uint32_t pivot_salt;        // xor on the vertex id before the tie-break hash of the degree rule (0 = none)
+    int32_t cta_deg = -1;       // top-down items above this degree are expanded by the whole block (-1 = never)
+    int64_t adj_len = 0;        // entries in node_idx and in r_node_idx (int4 probes stay below it)
+    int32_t vec_adj = 0;        // both adjacency arrays start on a 16-byte boundary (int4 probes allowed)
 };
+
+// Adjacency arrays of g as RoundArgs needs them: int4 probes only where both
+// arrays are 16-byte aligned, never past their m entries.
+__host__ inline void round_args_adjacency(RoundArgs& a, const int32_t* node_idx, const int32_t* r_node_idx,
+                                          int64_t m) {
+    a.adj_len = m;
+    a.vec_adj = ((reinterpret_cast<uintptr_t>(node_idx) | reinterpret_cast<uintptr_t>(r_node_idx)) & 15u) == 0;
+}
 
 __device__ __forceinline__ uint32_t pivot_hash(uint32_t v) {
     uint32_t x = v * 0x9E3779B1u;

@@ -5,20 +5,18 @@
 // transpose by scattering edges in source order (make_reverse_edges,
 // :193-287); on the device both become one sort of packed keys.
 //
-// Each pass handles 8 bits.  Tiles of 4,096 elements (256 threads x 16
-// elements, striped so that a round of 256 consecutive elements is one
-// element per thread in thread order):
-//  1. k_rs_hist: a shared-memory histogram of the digit per tile, written
-//     digit-major (counts[digit * tiles + tile]);
+// Each pass handles 8 bits, over tiles of 4,096 elements (256 threads x 16):
+//  1. k_rs_hist: a shared-memory histogram of the digit per tile (one per
+//     warp, summed), written digit-major (counts[digit * tiles + tile]);
 //  2. an exclusive scan of those counts gives every (digit, tile) its first
 //     output position;
-//  3. k_rs_scatter: each tile walks its 16 rounds in order; inside a round an
-//     element's slot is its digit's running slot plus the elements of that
-//     digit in earlier warps (per-warp counts in shared memory) plus the
-//     earlier lanes of its warp with that digit (__match_any_sync).  The tile
-//     is reordered by digit in shared memory first, then written out run by
-//     run, so the writes are coalesced.  Elements keep their input order
-//     within each digit, so the sort is stable.
+//  3. k_rs_scatter: each warp ranks its own contiguous segment of the tile
+//     (per-warp digit counts in shared memory, lanes of one digit found by
+//     ballots inside a round); a block scan over (digit, warp) turns the
+//     counts into slots.
+//     The tile is reordered by digit in shared memory first, then written
+//     out run by run, so the writes are coalesced.  Elements keep their
+//     input order within each digit, so the sort is stable.
 #include "scc_internal.cuh"
 #include "scc_sort.cuh"
 
@@ -108,86 +106,129 @@ static cudaError_t scan_excl(int32_t* a, int64_t L, int32_t* sums, cudaStream_t 
 }
 
 // ------------------------------------------------------------------ radix passes
+// Per-warp sub-histograms in shared memory (eight warps' atomics never meet
+// on one counter), summed per digit at the end of the tile.
 template <typename K>
 __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K* __restrict__ keys, int64_t m, int shift,
                                                         int32_t ntiles, int32_t* __restrict__ counts) {
-    __shared__ int32_t h[RS_BINS];
+    __shared__ int32_t h[RS_WARPS][RS_BINS];
+    const int wid = threadIdx.x >> 5;
     for (int32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        h[threadIdx.x] = 0;
+#pragma unroll
+        for (int w = 0; w < RS_WARPS; ++w) h[w][threadIdx.x] = 0;
         __syncthreads();
-        int64_t base = (int64_t)tile * RS_TILE;
+        const int64_t base = (int64_t)tile * RS_TILE;
+        K k[RS_ITEMS];
+#pragma unroll
         for (int r = 0; r < RS_ITEMS; ++r) {
             int64_t i = base + r * RS_THREADS + threadIdx.x;
-            if (i < m) atomicAdd(&h[(unsigned)(keys[i] >> shift) & (RS_BINS - 1)], 1);
+            k[r] = i < m ? keys[i] : (K)0;
         }
+#pragma unroll
+        for (int r = 0; r < RS_ITEMS; ++r)
+            if (base + r * RS_THREADS + threadIdx.x < m)
+                atomicAdd(&h[wid][(unsigned)(k[r] >> shift) & (RS_BINS - 1)], 1);
         __syncthreads();
-        counts[(int64_t)threadIdx.x * ntiles + tile] = h[threadIdx.x];
+        int32_t c = 0;
+#pragma unroll
+        for (int w = 0; w < RS_WARPS; ++w) c += h[w][threadIdx.x];
+        counts[(int64_t)threadIdx.x * ntiles + tile] = c;
         __syncthreads();
     }
 }
 
+// One tile per pass of the loop.  Warp w owns the tile's elements
+// [w * RS_SEG, (w + 1) * RS_SEG), read 32 consecutive ones per round, all
+// rounds' loads issued before any is ranked.  Its lanes rank them inside the
+// warp (earlier rounds first, then earlier lanes) against per-warp digit
+// counts in shared memory; the lanes of a round that share a digit are found
+// with eight ballots, one per digit bit.  One block scan over (digit, warp)
+// then gives each warp's slot for each digit; the tile is reordered by digit
+// in shared memory and written out run by run, each digit's output position
+// read once per tile into shared memory.  Within a digit the order is rounds,
+// lanes, warps -- the input order -- so the sort is stable.  Two blocks per
+// SM (registers capped at 128): a third of the time of one block per SM.
+#define RS_SEG (RS_TILE / RS_WARPS)
 template <typename K, bool VALS>
-__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K* __restrict__ kin, K* __restrict__ kout,
-                                                           const int32_t* __restrict__ vin,
-                                                           int32_t* __restrict__ vout, int64_t m, int shift,
-                                                           int32_t ntiles, const int32_t* __restrict__ offs) {
-    __shared__ int32_t run[RS_BINS];              // next tile-local slot of each digit
-    __shared__ int32_t start[RS_BINS];            // tile-local start of each digit
-    __shared__ int32_t wcnt[RS_WARPS][RS_BINS];
+__global__ void __launch_bounds__(RS_THREADS, 2) k_rs_scatter(const K* __restrict__ kin, K* __restrict__ kout,
+                                                              const int32_t* __restrict__ vin,
+                                                              int32_t* __restrict__ vout, int64_t m, int shift,
+                                                              int32_t ntiles, const int32_t* __restrict__ offs) {
+    __shared__ int32_t wcnt[RS_WARPS][RS_BINS];   // per-warp digit counts, then each warp's slot per digit
+    __shared__ int32_t dst[RS_BINS];              // output position of the digit's tile-local slot 0
     __shared__ K skey[RS_TILE];
     __shared__ int32_t sval[VALS ? RS_TILE : 1];
     __shared__ int32_t s_w[RS_WARPS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int j = threadIdx.x; j < RS_WARPS * RS_BINS; j += RS_THREADS) (&wcnt[0][0])[j] = 0;
+    const unsigned lt = (1u << lane) - 1u;
     for (int32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int64_t base = (int64_t)tile * RS_TILE;
         const int32_t cnt = (m - base < RS_TILE) ? (int32_t)(m - base) : RS_TILE;
-        // the tile's own histogram, and each digit's start inside the tile
-        run[threadIdx.x] = 0;
-        __syncthreads();
+        const int32_t seg = wid * RS_SEG;
+        K k[RS_ITEMS];
+        int32_t v[RS_ITEMS];
+        int32_t rank[RS_ITEMS];
+#pragma unroll
         for (int r = 0; r < RS_ITEMS; ++r) {
-            int32_t j = r * RS_THREADS + threadIdx.x;
-            if (j < cnt) atomicAdd(&run[(unsigned)(kin[base + j] >> shift) & (RS_BINS - 1)], 1);
+            const int32_t j = seg + r * 32 + lane;
+            k[r] = j < cnt ? kin[base + j] : (K)0;
+            v[r] = (VALS && j < cnt) ? vin[base + j] : 0;
+        }
+        const int32_t gofs = offs[(int64_t)threadIdx.x * ntiles + tile];    // digit threadIdx.x
+#pragma unroll
+        for (int q = lane; q < RS_BINS; q += 32) wcnt[wid][q] = 0;
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < RS_ITEMS; ++r) {
+            const bool valid = seg + r * 32 + lane < cnt;
+            const int d = (int)((unsigned)(k[r] >> shift) & (RS_BINS - 1));
+            unsigned peers = __ballot_sync(0xFFFFFFFFu, valid);
+#pragma unroll
+            for (int bit = 0; bit < 8; ++bit) {
+                const unsigned x = __ballot_sync(0xFFFFFFFFu, (d >> bit) & 1);
+                peers &= ((d >> bit) & 1) ? x : ~x;
+            }
+            // an invalid lane may see valid peers of digit d; it neither reads nor writes
+            const int leader = __ffs(peers) - 1;
+            int32_t cur = (valid && lane == leader) ? wcnt[wid][d] : 0;
+            cur = __shfl_sync(0xFFFFFFFFu, cur, leader < 0 ? lane : leader);
+            rank[r] = cur + __popc(peers & lt);
+            if (valid && lane == leader) wcnt[wid][d] = cur + __popc(peers);
+            __syncwarp();
         }
         __syncthreads();
-        int32_t tot = 0;
-        int32_t st0 = block_excl256(run[threadIdx.x], s_w, &tot);
-        start[threadIdx.x] = st0;
-        run[threadIdx.x] = st0;
-        __syncthreads();
-        // stable ranks: rounds in input order, warps in order, lanes in order
-        for (int r = 0; r < RS_ITEMS; ++r) {
-            int32_t j = r * RS_THREADS + threadIdx.x;
-            bool valid = j < cnt;
-            K k = valid ? kin[base + j] : (K)0;
-            int32_t v = (VALS && valid) ? vin[base + j] : 0;
-            int d = valid ? (int)((unsigned)(k >> shift) & (RS_BINS - 1)) : RS_BINS + lane;   // invalid lanes match nobody
-            unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
-            int lr = __popc(peers & ((1u << lane) - 1u));
-            bool leader = lane == __ffs(peers) - 1;
-            if (valid && leader) wcnt[wid][d] = __popc(peers);
-            __syncthreads();
-            if (valid) {
-                int32_t pre = 0;
-                for (int w = 0; w < wid; ++w) pre += wcnt[w][d];
-                int32_t pos = run[d] + pre + lr;
-                skey[pos] = k;
-                if (VALS) sval[pos] = v;
-            }
-            __syncthreads();
-            if (valid && leader) {
-                atomicAdd(&run[d], __popc(peers));
-                wcnt[wid][d] = 0;
-            }
-            __syncthreads();
+        // thread t owns digit t: the tile's start of the digit, then each warp's slot
+        {
+            int32_t c[RS_WARPS];
+            int32_t tot = 0;
+#pragma unroll
+            for (int w = 0; w < RS_WARPS; ++w) { c[w] = wcnt[w][threadIdx.x]; tot += c[w]; }
+            int32_t all = 0;
+            int32_t run = block_excl256(tot, s_w, &all);
+            dst[threadIdx.x] = gofs - run;
+#pragma unroll
+            for (int w = 0; w < RS_WARPS; ++w) { wcnt[w][threadIdx.x] = run; run += c[w]; }
         }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < RS_ITEMS; ++r) {
+            const int32_t j = seg + r * 32 + lane;
+            if (j < cnt) {
+                const int d = (int)((unsigned)(k[r] >> shift) & (RS_BINS - 1));
+                const int32_t pos = wcnt[wid][d] + rank[r];
+                skey[pos] = k[r];
+                if (VALS) sval[pos] = v[r];
+            }
+        }
+        __syncthreads();
         // the tile leaves in digit order: consecutive threads write consecutive
         // slots of each digit's run
+#pragma unroll 4
         for (int32_t j = threadIdx.x; j < cnt; j += RS_THREADS) {
-            K k = skey[j];
-            int d = (int)((unsigned)(k >> shift) & (RS_BINS - 1));
-            int64_t pos = (int64_t)offs[(int64_t)d * ntiles + tile] + (j - start[d]);
-            kout[pos] = k;
+            const K kk = skey[j];
+            const int d = (int)((unsigned)(kk >> shift) & (RS_BINS - 1));
+            const int64_t pos = (int64_t)dst[d] + j;
+            kout[pos] = kk;
             if (VALS) vout[pos] = sval[j];
         }
         __syncthreads();

@@ -305,6 +305,7 @@ extern "C" int scc_state_set_tuning(scc_state* s, const scc_tuning* t) {
     if (t->pivot_salt != 0) s->tune.pivot_salt = t->pivot_salt == -1 ? 0 : t->pivot_salt;
     if (t->tail_live != 0) s->tune.tail_live = t->tail_live > 0 ? t->tail_live : -1;
     if (t->tail_class > 0) s->tune.tail_class = t->tail_class;
+    if (t->cta_deg != 0) s->tune.cta_deg = t->cta_deg > 0 ? t->cta_deg : -1;
     return SCC_OK;
 }
 

@@ -30,6 +30,7 @@ static const int32_t K_HUGE[] = {1024, 4096, 16384};              // edge-parall
 static const int32_t K_TILE[] = {-1, 1 << 18, 1 << 20};           // tile drain from this many live vertices
 static const int32_t K_SPAN[] = {2048, 16384};                    // smallest tile
 static const int32_t K_TAIL[] = {-1, 1 << 18, 1 << 20};           // one-launch tail from this many live vertices
+static const int32_t K_CTA[] = {-1, 256, 1024};                   // block-wide expansion above this degree
 
 static scc_tuning candidate(uint64_t& rng) {
     auto pick = [&](const int32_t* v, int k) {
@@ -49,6 +50,7 @@ static scc_tuning candidate(uint64_t& rng) {
     t.pivot_salt = 0;
     t.tail_live = pick(K_TAIL, 3);
     t.tail_class = 1 << 16;
+    t.cta_deg = pick(K_CTA, 3);
     return t;
 }
 

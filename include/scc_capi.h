@@ -184,10 +184,13 @@ typedef struct scc_tuning {
                                      finished in one launch, a block per class; negative = never (the
                                      default) */
     int32_t tail_class;           /* ... provided no class has more vertices than this (1 << 16) */
+    int32_t cta_deg;              /* top-down items above this degree (up to huge_deg) are expanded by a whole
+                                     block, their adjacency staged in shared memory by bulk copies; negative =
+                                     never */
 } scc_tuning;
 int scc_state_get_tuning(scc_state* s, scc_tuning* t);
-/* Fields <= 0 keep their current value, except tile_min_live and tail_live,
- * where a negative value turns that path off, and pivot_salt, which any
+/* Fields <= 0 keep their current value, except tile_min_live, tail_live and
+ * cta_deg, where a negative value turns that path off, and pivot_salt, which any
  * non-zero value sets (and -1 resets to 0). */
 int scc_state_set_tuning(scc_state* s, const scc_tuning* t);
 /* Autotuner: successive halving over the tunables with a budget of max_trials full
