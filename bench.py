@@ -415,9 +415,10 @@ def bench_serving(args, local_rank, batches_n=None, sustain_n=None):
     phase's last 100 admitted batches: the device busy about a third of the
     time, since the service time is heavy-tailed and queueing delay grows with
     its second moment), where p50/p99 describe the system rather than the
-    length of the run.  A check waits for the batches before it and copies the
-    graph out; the arrival clock stops meanwhile (rates and wall times leave
-    the pauses out).  Returns the JSON line."""
+    length of the run.  A check waits for the batches before it (serving
+    time) and then copies the graph and labels out with the device idle; the
+    clocks stop for the copy (rates and wall times leave it out).  Returns the
+    JSON line."""
     import multiprocessing as mp
     from concurrent.futures import ProcessPoolExecutor
     import torch
@@ -469,11 +470,12 @@ def bench_serving(args, local_rank, batches_n=None, sustain_n=None):
                 pending.append((rid, edges))
             counter["batches"] += 1
             if counter["batches"] % 100 == 0:
-                # the check needs the session idle at this batch; the arrival
-                # clock stops meanwhile, so no burst of late arrivals follows it
-                tp = time.perf_counter()
+                # the check needs the session idle at this batch: waiting for
+                # the queue is serving time; the copy-out that follows leaves
+                # the device idle, so the clocks stop for it
                 results += [(sv.wait(r), e) for r, e in pending]
                 pending = []
+                tp = time.perf_counter()
                 cb, ca, _, _ = sv.session_csr(sid)
                 checks.append(pool.submit(_tarjan_equal, cb, ca, sv.labels(sid)))
                 t0 += time.perf_counter() - tp

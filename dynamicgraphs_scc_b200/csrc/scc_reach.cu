@@ -917,18 +917,23 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
         s->traversal_steps++;
         if (!synced) SCC_TRY(scc_sync_counters(s));
         int32_t next = s->h_ctr[CTR_QLEN];
+        // a frontier of few items may still hold hubs: it counts as narrow
+        // only while its edges stay under the drain's hand-back bound, else
+        // the drain would take it, grow past the bound and hand it back
+        bool edges_small = true;
         if (bottom_up) {
             bottom_up = (int64_t)next * s->tune.bu_div > live2;
         } else {
             unsigned long long fe = *reinterpret_cast<unsigned long long*>(s->h_ctr + CTR_EDGES);
             bottom_up = fe * (unsigned long long)s->tune.bu_alpha > live_edges;
+            edges_small = fe <= (unsigned long long)a.async_bail;
         }
         if (scc_trace_on()) {
             double t1 = now_ms();
             fprintf(stderr, "[scc] reach %s in=%d out=%d %.3f ms\n", mode, qlen, next, t1 - t0);
             t0 = t1;
         }
-        narrow = (!bottom_up && next <= s->tune.async_max) ? narrow + 1 : 0;
+        narrow = (!bottom_up && next <= s->tune.async_max && edges_small) ? narrow + 1 : 0;
         qlen = next;
         int32_t* t = qin; qin = qout; qout = t;
     }
