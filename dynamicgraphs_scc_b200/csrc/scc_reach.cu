@@ -894,12 +894,21 @@ int scc_impl_reach(const scc_graph* g, scc_state* s, RoundArgs& a, int32_t qlen)
             SCC_TRY(scc_zero_counters(s, CTR_QLEN, 1));
             SCC_TRY(scc_zero_counters(s, CTR_SPARE4, 1));
             SCC_TRY(scc_zero_counters(s, CTR_EDGES, 2));
-            if (a.cta_deg > 0 && a.cta_deg < a.huge_deg)
-                k_reach_level<true><<<scc_blocks((int64_t)qlen, REACH_THREADS, 148 * 8), REACH_THREADS, 0, s->stream>>>(
-                    a, qin, qlen, qout, s->hq);
+            const int lblocks = scc_blocks((int64_t)qlen, REACH_THREADS, 148 * 8);
+            RoundArgs la = a;
+            bool block_bucket = a.cta_deg > 0 && a.cta_deg < a.huge_deg;
+            if (block_bucket && lblocks < 148) {
+                // a level of fewer blocks than SMs would expand each mid-degree
+                // item in one block while most SMs idle: those items go
+                // edge-parallel over the whole GPU instead (the pivot's own
+                // lists, the first levels after it)
+                la.huge_deg = a.cta_deg;
+                block_bucket = false;
+            }
+            if (block_bucket)
+                k_reach_level<true><<<lblocks, REACH_THREADS, 0, s->stream>>>(la, qin, qlen, qout, s->hq);
             else
-                k_reach_level<false><<<scc_blocks((int64_t)qlen, REACH_THREADS, 148 * 8), REACH_THREADS, 0, s->stream>>>(
-                    a, qin, qlen, qout, s->hq);
+                k_reach_level<false><<<lblocks, REACH_THREADS, 0, s->stream>>>(la, qin, qlen, qout, s->hq);
             SCC_LAUNCHED(s);
             SCC_TRY(scc_sync_counters(s));
             if (s->h_ctr[CTR_ERROR]) return scc_check_device_error(s);

@@ -6,7 +6,9 @@ oracle's Tarjan.
   by 1-D bulk copies, chunk by chunk, two buffers deep.  The cases force it on
   (low cta_deg, bottom-up off so every level is top-down) for mid-degree hubs,
   a list of several chunks that starts off a 16-byte boundary, and lists of
-  every length modulo 4 (the unstaged tail).
+  every length modulo 4 (the unstaged tail).  A level of fewer blocks than
+  SMs sends the same items edge-parallel over the whole GPU instead, so the
+  small cases cover that route and a wide level covers the block bucket.
 * Bottom-up probes: both directions at once, an aligned int4 chunk of each
   list per probe; rounds over one class and over many classes, lists that
   start at every offset modulo 4, and a list that ends at the last entry of
@@ -59,6 +61,13 @@ def _mid_hubs(seed, n=40000, hubs=300):
 def test_block_expansion_mid_degree_hubs(gpu, cta_deg):
     n, s, d = _mid_hubs(5)
     _check(n, s, d, cta_deg=cta_deg, **TOP_DOWN)
+
+
+def test_block_expansion_wide_level(gpu):
+    # levels of more than 148 blocks' worth of items (37,888): the block
+    # bucket proper, beside the edge-parallel route of the first levels
+    n, s, d = _mid_hubs(7, n=300000, hubs=2000)
+    _check(n, s, d, methods=(2,), cta_deg=256, **TOP_DOWN)
 
 
 def test_block_expansion_default_traversal(gpu):
