@@ -151,7 +151,7 @@ struct scc_state {
     // resident warps in the drain mean less contention on its queue)
     // (the tile drain and the one-launch tail are off by default: measured
     // slower than the shared-queue drain and the round engine on C2)
-    scc_tuning tune = {14, 24, 1 << 14, 1, 16, 1, 4096, -1, 2048, 0, -1, 1 << 16, 256};
+    scc_tuning tune = {14, 24, 1 << 14, 1, 16, 1, 4096, -1, 2048, 0, 1 << 16, 1024, 256};
 
     // kernel ledger (scc_state_profile): device time and algorithmic bytes of
     // the asynchronous reachability drain, timed with events on `stream`

@@ -29,7 +29,7 @@ static const int32_t K_BLOCKS[] = {1, 2};                         // drain block
 static const int32_t K_HUGE[] = {1024, 4096, 16384};              // edge-parallel hub expansion above this degree
 static const int32_t K_TILE[] = {-1, 1 << 18, 1 << 20};           // tile drain from this many live vertices
 static const int32_t K_SPAN[] = {2048, 16384};                    // smallest tile
-static const int32_t K_TAIL[] = {-1, 1 << 18, 1 << 20};           // one-launch tail from this many live vertices
+static const int32_t K_TAIL[] = {-1, 1 << 14, 1 << 16};           // one-launch tail from this many live vertices
 static const int32_t K_CTA[] = {-1, 256, 1024};                   // block-wide expansion above this degree
 
 static scc_tuning candidate(uint64_t& rng) {
@@ -49,7 +49,7 @@ static scc_tuning candidate(uint64_t& rng) {
     t.tile_min_span = pick(K_SPAN, 2);
     t.pivot_salt = 0;
     t.tail_live = pick(K_TAIL, 3);
-    t.tail_class = 1 << 16;
+    t.tail_class = 1024;
     t.cta_deg = pick(K_CTA, 3);
     return t;
 }

@@ -181,9 +181,8 @@ typedef struct scc_tuning {
     int32_t pivot_salt;           /* xor on vertex ids before the degree rule's tie-break hash (0): picks
                                      another of the equally good pivots; changes speed, never labels */
     int32_t tail_live;            /* from the second recursion round on, at most this many live vertices are
-                                     finished in one launch, a block per class; negative = never (the
-                                     default) */
-    int32_t tail_class;           /* ... provided no class has more vertices than this (1 << 16) */
+                                     finished in one launch, a block per class (65536); negative = never */
+    int32_t tail_class;           /* ... provided no class has more vertices than this (1024) */
     int32_t cta_deg;              /* top-down items above this degree (up to huge_deg) are expanded by a whole
                                      block, their adjacency staged in shared memory by bulk copies; negative =
                                      never */
