@@ -774,6 +774,8 @@ def main():
                     help="skip the secondary configurations of the default run (R-MAT s24, learned pivot, streaming)")
     ap.add_argument("--extra-batches", type=int, default=1000, help="streaming batches measured in the default run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default="",
+                    help="comma-separated scc_tuning fields for the engine arm, e.g. bu_alpha=1,cta_deg=256")
     ap.add_argument("--ref-sample", action="store_true",
                     help="reference arm: time the 1/16 sample instead of the full configuration")
     args = ap.parse_args()
@@ -855,6 +857,9 @@ def main():
     g = workload_graph(kw, local_rank)
     n, m = g.num_nodes(), g.num_edges()
     st = State(g)
+    tuning = {k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(",") if kv)}
+    if tuning:
+        st.set_tuning(**tuning)
     if model is not None:
         st.set_pivot_model(model)
         st.set_tuning(tail_live=-1)        # both forms without the one-launch tail, which learned pivots do not use
@@ -1042,7 +1047,8 @@ def main():
         "config": {"workload": WORKLOAD_NAMES[args.workload], "params": kw, "n": n, "m": m, "method": 2,
                    "pivot": ("learned (MLP 8-64-64-1, BF16 weights, re-ranks the in*out candidates)" if learned
                              else "max in*out degree"),
-                   "parallelism": f"replicas x{world}", "l2": "inputs (CSR+transpose) > L2; no flush"},
+                   "parallelism": f"replicas x{world}", "l2": "inputs (CSR+transpose) > L2; no flush",
+                   **({"tuning": tuning} if tuning else {})},
         "roofline": kernel_roofline,
         "roofline_step": {"bound": "hbm", "scope": "whole step (16M+20N+8 algorithmic bytes)",
                           "achieved": round(achieved, 2), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
