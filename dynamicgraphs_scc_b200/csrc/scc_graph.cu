@@ -402,13 +402,28 @@ __global__ void k_runs_scatter(int32_t n, RunBounds rb, const int32_t* __restric
     }
 }
 
+// Source id of every edge of vertices [s0, s1): a lane per vertex, and the
+// whole warp for a list of more than 32 entries (a warp per vertex spent most
+// of its lanes idle on a grid's lists of one or two entries).
 __global__ void k_expand_sources_range(int32_t s0, int32_t s1, const int32_t* __restrict__ begin,
                                        int32_t* __restrict__ src) {
-    int lane = threadIdx.x & 31;
-    for (int64_t w = s0 + ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5); w < s1;
-         w += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        int32_t b = begin[w], e = begin[w + 1];
-        for (int32_t k = b + lane; k < e; k += 32) src[k] = (int32_t)w;
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = s0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x - lane; base < s1; base += stride) {
+        const int64_t w = base + lane;             // base is warp-uniform
+        int32_t b = 0, e = 0;
+        if (w < s1) { b = begin[w]; e = begin[w + 1]; }
+        const bool big = e - b > 32;
+        if (!big)
+            for (int32_t k = b; k < e; ++k) src[k] = (int32_t)w;
+        unsigned m = __ballot_sync(0xFFFFFFFFu, big);
+        while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const int32_t bb = __shfl_sync(0xFFFFFFFFu, b, l), be = __shfl_sync(0xFFFFFFFFu, e, l);
+            const int32_t wv = (int32_t)__shfl_sync(0xFFFFFFFFu, (int32_t)w, l);
+            for (int32_t k = bb + lane; k < be; k += 32) src[k] = wv;
+        }
     }
 }
 
@@ -489,7 +504,7 @@ static int upload_pipelined(scc_graph* g, const int32_t* begin, const int32_t* n
             SCC_CUDA(cudaMemsetAsync(oj, 0, sizeof(int32_t) * ((size_t)n + 1), evs.cs));
             continue;
         }
-        k_expand_sources_range<<<scc_blocks((int64_t)(sv[j + 1] - sv[j]) * 32, 256, 148 * 64), 256, 0, evs.cs>>>(
+        k_expand_sources_range<<<scc_blocks((int64_t)(sv[j + 1] - sv[j]), 256, 148 * 64), 256, 0, evs.cs>>>(
             sv[j], sv[j + 1], g->begin, (int32_t*)src.p);
         SCC_CUDA(cudaPeekAtLastError());
         SCC_TRY(scc_impl_sort_pairs_u32(reinterpret_cast<const uint32_t*>(g->node_idx + e0), (uint32_t*)keys.p + e0,

@@ -113,6 +113,26 @@ def test_very_long_cycle_completes(gpu):
     st.free(); g.free()
 
 
+def test_several_long_chains_at_once(gpu):
+    # four disjoint cycles of 0.6-1.2 M vertices: the global step walks one
+    # (its FW and BW chains in two warps), then one round walks the other
+    # three at once, six single-hop chains of different lengths in different
+    # warps while idle warps run out their wait bound; every chain must still
+    # reach its end, and the chains that end first must not end the drain
+    lens = [1200000, 1000000, 800000, 600000]
+    starts = np.concatenate([[0], np.cumsum(lens)[:-1]])
+    s = np.concatenate([st + np.arange(L) for st, L in zip(starts, lens)]).astype(np.int32)
+    d = np.concatenate([st + (np.arange(L) + 1) % L for st, L in zip(starts, lens)]).astype(np.int32)
+    n = int(sum(lens))
+    g = Graph.from_edges(n, s, d)
+    st = State(g)
+    r = st.run(2)
+    assert r["num_sccs"] == 4
+    exp = np.repeat(starts, lens).astype(np.int32)
+    assert np.array_equal(st.canonical_labels(), exp)
+    st.free(); g.free()
+
+
 def _hub_graph():
     rng = np.random.default_rng(51)
     leaves = 200000
