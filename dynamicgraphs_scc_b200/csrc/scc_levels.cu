@@ -15,8 +15,8 @@
 // that are never released (on or behind a cycle, when the labels are not the
 // SCCs of the graph) keep the largest level + 1 of their released
 // predecessors, or 0 -- what the reference's queue leaves them.
-#include <cub/cub.cuh>
 #include "scc_internal.cuh"
+#include "scc_sort.cuh"
 
 #define LEVEL_Q 256          // per-warp queue of released nodes awaiting expansion
 #define LEVEL_HUB 4096       // a released node with more out-edges is expanded over the whole grid
@@ -315,7 +315,7 @@ extern "C" int scc_affected_levels(const scc_graph* dag, const int32_t* levels, 
     SCC_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
     cudaStream_t st = s.st;
     const int32_t L = max_level + 1;
-    Buf lab, lev, src, dst, diff, out, bad, tmp;
+    Buf lab, lev, src, dst, diff, out, bad;
     SCC_TRY(get(lab, sizeof(int32_t) * (size_t)n, st));
     SCC_TRY(get(lev, sizeof(int32_t) * (size_t)dag->n, st));
     SCC_TRY(get(src, sizeof(int32_t) * (size_t)n_ins, st));
@@ -336,10 +336,7 @@ extern "C" int scc_affected_levels(const scc_graph* dag, const int32_t* levels, 
                                                                 max_level, diff.as<int32_t>(), bad.as<int>());
         SCC_CUDA(cudaPeekAtLastError());
     }
-    size_t tbytes = 0;
-    SCC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tbytes, diff.as<int32_t>(), out.as<int32_t>(), L, st));
-    SCC_TRY(get(tmp, tbytes, st));
-    SCC_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tbytes, diff.as<int32_t>(), out.as<int32_t>(), L, st));
+    SCC_TRY(scc_impl_scan_i32(diff.as<int32_t>(), out.as<int32_t>(), L, true, st));
     k_count_zero<<<scc_blocks(L), SCC_THREADS, 0, st>>>(L, out.as<int32_t>(), bad.as<int32_t>() + 1);
     SCC_CUDA(cudaPeekAtLastError());
     int32_t h[2] = {0, 0};

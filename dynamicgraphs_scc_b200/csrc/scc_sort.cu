@@ -321,6 +321,28 @@ int scc_impl_sort_pairs_u32(const uint32_t* keys_in, uint32_t* keys_out, const i
     return radix_sort<uint32_t>(keys_in, keys_out, vals_in, vals_out, m, bits, st, scratch);
 }
 
+__global__ void k_add_i32(const int32_t* __restrict__ in, int32_t* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] += in[i];
+}
+
+int scc_impl_scan_i32(const int32_t* in, int32_t* out, int64_t n, bool inclusive, cudaStream_t st) {
+    SCC_REQUIRE(n >= 0 && n < (1LL << 31), SCC_ERR_INVALID, "scan of %lld elements", (long long)n);
+    SCC_REQUIRE(!(inclusive && in == out), SCC_ERR_INVALID, "inclusive scan in place");
+    if (n == 0) return SCC_OK;
+    if (in != out) SCC_CUDA(cudaMemcpyAsync(out, in, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    void* sums = nullptr;
+    SCC_CUDA(scc_impl_malloc_async(&sums, sizeof(int32_t) * (size_t)(n / SCAN_CHUNK + 2), st));
+    cudaError_t e = scan_excl(out, n, (int32_t*)sums, st);
+    if (e == cudaSuccess && inclusive) {
+        k_add_i32<<<scc_blocks(n, RS_THREADS, 148 * 8), RS_THREADS, 0, st>>>(in, out, n);
+        e = cudaPeekAtLastError();
+    }
+    cudaFreeAsync(sums, st);
+    SCC_CUDA(e);
+    return SCC_OK;
+}
+
 int scc_impl_sort_keys_u64(const unsigned long long* keys_in, unsigned long long* keys_out, int64_t m, int bits,
                            cudaStream_t st) {
     return radix_sort<unsigned long long>(keys_in, keys_out, nullptr, nullptr, m, bits, st, nullptr);

@@ -20,12 +20,10 @@
 //     every merged SCC lies in R = FW(those v) and BW(those u).  R is a union
 //     of classes closed under strong connectivity; SCCs are recomputed inside
 //     R only.
-#include <cub/block/block_scan.cuh>
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
 #include <algorithm>
 #include <string.h>
 #include "scc_round.cuh"
+#include "scc_sort.cuh"
 
 // ------------------------------------------------------------------ kernels
 __global__ void k_upd_keys(int64_t k, const int32_t* __restrict__ a, const int32_t* __restrict__ b, int32_t n,
@@ -218,26 +216,23 @@ static void release_graph_arrays(scc_graph* g, cudaStream_t st) {
 // keys (a<<32|b) sorted ascending into out (k entries); invalid ids flagged in *bad.
 static int sorted_keys(int64_t k, const int32_t* d_a, const int32_t* d_b, int32_t n, cudaStream_t st,
                        DevBuf& out, int* d_bad) {
-    DevBuf tmpk, tmp;
+    DevBuf tmpk;
     SCC_TRY(alloc(out, sizeof(unsigned long long) * (size_t)k, st));
     SCC_TRY(alloc(tmpk, sizeof(unsigned long long) * (size_t)k, st));
     if (k == 0) return SCC_OK;
     k_upd_keys<<<scc_blocks(k), SCC_THREADS, 0, st>>>(k, d_a, d_b, n, tmpk.as<unsigned long long>(), d_bad);
     SCC_CUDA(cudaPeekAtLastError());
-    size_t bytes = 0;
-    SCC_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, bytes, tmpk.as<unsigned long long>(), out.as<unsigned long long>(),
-                                            (int)k, 0, 64, st));
-    SCC_TRY(alloc(tmp, bytes, st));
-    SCC_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, bytes, tmpk.as<unsigned long long>(), out.as<unsigned long long>(),
-                                            (int)k, 0, 64, st));
-    return SCC_OK;
+    // a < n in the high word: the bits above 32 + log2(n) are zero
+    int hb = 1;
+    while (hb < 31 && (1LL << hb) < (int64_t)n) hb++;
+    return scc_impl_sort_keys_u64(tmpk.as<unsigned long long>(), out.as<unsigned long long>(), k, 32 + hb, st);
 }
 
 // Merge one side (off/adj) with sorted deleted and inserted keys; returns new arrays.
 static int merge_side(int32_t n, int64_t m, const int32_t* off, const int32_t* adj, const unsigned long long* del,
                       int64_t kdel, const unsigned long long* ins, int64_t kins, cudaStream_t st, int32_t** new_off,
                       int32_t** new_adj, int64_t* new_m) {
-    DevBuf dead, ndead, insb, deg, tmp, kp;
+    DevBuf dead, ndead, insb, deg, kp;
     SCC_TRY(alloc(kp, sizeof(int32_t) * (size_t)(m > 0 ? m : 1), st));
     SCC_TRY(alloc(dead, (size_t)(m > 0 ? m : 1), st));
     SCC_TRY(alloc(ndead, sizeof(int32_t) * (size_t)n, st));
@@ -258,10 +253,10 @@ static int merge_side(int32_t n, int64_t m, const int32_t* off, const int32_t* a
     }
     int32_t* noff = nullptr;
     SCC_CUDA(scc_impl_malloc_async((void**)&noff, sizeof(int32_t) * ((size_t)n + 1), st));
-    size_t bytes = 0;
-    SCC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, deg.as<int32_t>(), noff, n + 1, st));
-    SCC_TRY(alloc(tmp, bytes, st));
-    SCC_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, bytes, deg.as<int32_t>(), noff, n + 1, st));
+    {
+        int rc = scc_impl_scan_i32(deg.as<int32_t>(), noff, (int64_t)n + 1, false, st);
+        if (rc != SCC_OK) { cudaFreeAsync(noff, st); return rc; }
+    }
     int32_t nm = 0;
     SCC_CUDA(cudaMemcpyAsync(&nm, noff + n, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     SCC_CUDA(cudaStreamSynchronize(st));
@@ -521,8 +516,7 @@ __global__ void __launch_bounds__(SCC_THREADS) k_cond_cross(int32_t m, int64_t c
                                                             const int32_t* __restrict__ owner,
                                                             int32_t* __restrict__ out_src, int32_t* __restrict__ out_dst,
                                                             int32_t* __restrict__ count) {
-    using Scan = cub::BlockScan<int, SCC_THREADS>;
-    __shared__ typename Scan::TempStorage scan_tmp;
+    __shared__ int32_t scan_w[SCC_THREADS / 32];
     __shared__ int32_t s_off[COND_TILE_V + 1];
     __shared__ int32_t s_lab[COND_TILE_V];
     __shared__ int32_t s_base;
@@ -580,8 +574,8 @@ __global__ void __launch_bounds__(SCC_THREADS) k_cond_cross(int32_t m, int64_t c
             for (int j = 0; j < COND_ITEMS; j++)
                 if (k0 + j < e1 && sl[j] != d[j]) keep |= 1 << j;
         }
-        int pre, total;
-        Scan(scan_tmp).ExclusiveSum(__popc(keep), pre, total);
+        int32_t total = 0;
+        const int32_t pre = scc_block_excl_sum256(__popc(keep), scan_w, &total);
         if (threadIdx.x == 0 && total > 0) s_base = atomicAdd(count, total);
         __syncthreads();
         if (keep) {
