@@ -644,6 +644,9 @@ __global__ void __launch_bounds__(ASYNC_THREADS, 1) k_reach_async(RoundArgs a, i
             int32_t got = 0, base = 0;
             if (lane == 0) {
                 int32_t t = ld_volatile(tail), h = ld_volatile(head);
+                // a queue that overflowed (its error already recorded by the
+                // spill) is read no further than its capacity
+                if ((int64_t)t > qcap) t = (int32_t)qcap;
                 if (h < t) {
                     int32_t k = min(32, t - h);
                     if (atomicCAS(head, h, h + k) == h) { got = k; base = h; }
