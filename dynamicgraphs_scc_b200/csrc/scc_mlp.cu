@@ -168,7 +168,11 @@ __global__ void k_pivot_log(RoundArgs a, const unsigned long long* __restrict__ 
 // Candidates of the learned choice: vertices whose in x out degree is within a
 // factor CAND_DIV of the best of their class (slot_key holds the degree keys).
 // The network re-ranks these; a class's degree pivot is always among them.
-#define CAND_DIV 4ull
+// CAND_DIV 1 keeps the vertices tied at the best: on C2 a window of 4x let the
+// network pick grid vertices outside the grid's giant SCC, each miss one more
+// 17-18 ms wave (learned/plain 0.50-0.82 over three trainings; 2x: 0.54-0.60;
+// ties only: 0.86-0.99), while C3 measured the same with all three (0.91-0.93).
+#define CAND_DIV 1ull
 __global__ void k_pivot_candidates(RoundArgs a, int32_t* __restrict__ cand, int32_t* __restrict__ ncand) {
     int lane = threadIdx.x & 31;
     int64_t limit = (((int64_t)a.live_count + 31) / 32) * 32;
