@@ -165,6 +165,19 @@ def hub_edges(hubs_n, hubs, hub_deg, seed):
     return hubs_n, np.concatenate(s), np.concatenate(d)
 
 
+def parse_tuning(text):
+    """"bu_alpha=1,cta_deg=256" -> {"bu_alpha": 1, "cta_deg": 256}; "" -> {}."""
+    out = {}
+    for kv in text.split(","):
+        if not kv.strip():
+            continue
+        k, sep, v = kv.partition("=")
+        if not sep:
+            raise ValueError(f"tuning entry {kv!r} is not key=value")
+        out[k.strip()] = int(v)
+    return out
+
+
 def workload_edges(kw):
     """Seeded edge list (n, src, dst) of a workload, on the host."""
     from dynamicgraphs_scc_b200 import generate_edges_host
@@ -857,7 +870,7 @@ def main():
     g = workload_graph(kw, local_rank)
     n, m = g.num_nodes(), g.num_edges()
     st = State(g)
-    tuning = {k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(",") if kv)}
+    tuning = parse_tuning(args.tuning)
     if tuning:
         st.set_tuning(**tuning)
     if model is not None:
