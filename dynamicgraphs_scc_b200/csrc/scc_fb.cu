@@ -233,8 +233,9 @@ int scc_impl_fb_round(const scc_graph* g, scc_state* s, int32_t only_color, int3
         k_pivot_key<<<blocks, SCC_THREADS, 0, s->stream>>>(a, s->hq, nclass, one_class ? 1 : 0);
         SCC_LAUNCHED(s);
         const bool learned = s->pivot_mode == SCC_PIVOT_LEARNED && s->pivot_model;
-        if (learned || s->log_cap > 0) SCC_TRY(scc_impl_pivot_prepare(g, s, a, learned, s->qa));
-        if (!learned) {
+        bool seeded = false;
+        if (learned || s->log_cap > 0) SCC_TRY(scc_impl_pivot_prepare(g, s, a, learned, s->qa, &seeded));
+        if (!seeded) {
             k_pivot_seed<<<scc_blocks(s->live_count, SCC_THREADS, 148 * 4), SCC_THREADS, 0, s->stream>>>(a, s->hq, nclass,
                                                                                                      s->qa);
             SCC_LAUNCHED(s);

@@ -652,13 +652,16 @@ static unsigned tc_blocks(int64_t count) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, 148LL * 4));
 }
 
-int scc_impl_pivot_prepare(const scc_graph* g, scc_state* s, RoundArgs& a, bool learned, int32_t* q) {
+int scc_impl_pivot_prepare(const scc_graph* g, scc_state* s, RoundArgs& a, bool learned, int32_t* q, bool* seeded) {
     (void)g;
+    *seeded = false;
     const bool logging = s->log_cap > 0;
     if ((!learned && !logging) || a.live_count <= 0) return SCC_OK;
     unsigned blocks = scc_blocks(a.live_count);
-    k_class_sizes<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
-    SCC_LAUNCHED(s);
+    if (logging) {
+        k_class_sizes<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
+        SCC_LAUNCHED(s);
+    }
     const unsigned long long* cr = s->cnt_valid ? s->cnt : nullptr;
     if (logging) {
         LogArgs lg;
@@ -677,6 +680,15 @@ int scc_impl_pivot_prepare(const scc_graph* g, scc_state* s, RoundArgs& a, bool 
     SCC_TRY(scc_zero_counters(s, CTR_SPARE1, 1));
     k_pivot_candidates<<<blocks, SCC_THREADS, 0, s->stream>>>(a, s->pivot_cand, ncand);
     SCC_LAUNCHED(s);
+    // every listed class's degree pivot is one of its candidates, so no more
+    // candidates than classes (CTR_SPARE4, counted by k_pivot_key) means no
+    // class has a choice: the degree pivots are the learned ones, unscored
+    SCC_TRY(scc_sync_counters(s));
+    if (s->h_ctr[CTR_SPARE1] <= s->h_ctr[CTR_SPARE4]) return SCC_OK;
+    if (!logging) {
+        k_class_sizes<<<blocks, SCC_THREADS, 0, s->stream>>>(a);
+        SCC_LAUNCHED(s);
+    }
     k_cand_features<<<blocks, SCC_THREADS, 0, s->stream>>>(a, cr, s->pivot_cand, ncand, (uint4*)s->pivot_x);
     SCC_LAUNCHED(s);
     k_mlp_score_tc<<<tc_blocks(a.live_count), TC_ROWS, TC_SMEM, s->stream>>>(
@@ -688,6 +700,7 @@ int scc_impl_pivot_prepare(const scc_graph* g, scc_state* s, RoundArgs& a, bool 
     SCC_LAUNCHED(s);
     k_cand_pick<<<blocks, SCC_THREADS, 0, s->stream>>>(a, s->pivot_cand, ncand, s->pivot_score, q);
     SCC_LAUNCHED(s);
+    *seeded = true;
     return SCC_OK;
 }
 

@@ -79,7 +79,9 @@ __device__ __forceinline__ void seed_pivot(const RoundArgs& a, int32_t v, int32_
 // slot_key: class sizes, training records when logging is on, and, when
 // `learned`, the pivot of every class chosen by the network among the class's
 // degree candidates and seeded into q (instead of the degree pick).
-int scc_impl_pivot_prepare(const scc_graph* g, scc_state* s, RoundArgs& a, bool learned, int32_t* q);
+// *seeded: whether q was seeded; false when no class has a second candidate
+// (the network would have no choice), and the caller seeds the degree pivots.
+int scc_impl_pivot_prepare(const scc_graph* g, scc_state* s, RoundArgs& a, bool learned, int32_t* q, bool* seeded);
 
 // Claim w for direction `dir` inside colour c; true if this thread claimed it.
 __device__ __forceinline__ bool visit(const RoundArgs& a, int32_t w, int32_t c, int dir) {
